@@ -1,0 +1,585 @@
+// Fused particle-step kernel: n_steps outer steps of GLIDE's static step body
+// per launch, one thread per particle, particle state held in registers
+// across steps.
+//
+// Per step (reference: src/lpdm/turbulence/hanna.py:898-1068 and the runtime
+// body src/lpdm/main.py:1396-1477):
+//   active mask -> RK2 midpoint advection through trilinear wind (two
+//   snapshots lerped by alpha) -> bilinear surface fields (lerped) -> Obukhov
+//   length / w* -> Hanna column turbulence at z_eval and z_eval +- 1 m (free
+//   troposphere override from the support bricks) -> well-mixed + density
+//   drift -> per-particle exact-OU substeps (clip, displacement, reflection)
+//   -> meander OU -> [post] time-ago bin, warp-aggregated footprint atomic,
+//   escape kill.
+//
+// Met is read from the packed per-window bricks (window_pack.cu): the wind
+// brick holds u, v, w of both snapshots in one 32-byte (float32) or 16-byte
+// (bf16/fp16) cell record, the support brick the six per-window support
+// channels, so every trilinear corner is one or two 128-bit loads.
+#include <cmath>
+#include <cstdio>
+
+#include "common.cuh"
+#include "glide_internal.h"
+
+namespace glide {
+
+template <typename T> struct Scales {
+    static constexpr float sp = 1.0f;    // stored sp  = sp  / sp
+    static constexpr float drho = 1.0f;  // stored drho = drho * drho_store
+};
+template <> struct Scales<__half> {
+    static constexpr float sp = 100.0f;
+    static constexpr float drho = 1e-4f;
+};
+
+struct StepDev {
+    int64_t n;
+    float* lon; float* lat; float* z; float* weight; int64_t ps;
+    float* up; float* vp; float* wp; float* um; float* vm;
+    const float* rel_off; const float* win_end_off; const int32_t* release_idx;
+    uint8_t* alive; const uint8_t* active_mask;
+    float sim_length;
+    const void* wind; const void* surf; const void* support;
+    GridDev g;
+    float substep_c; int max_substeps; float z_ubl;
+    int floors; int sl_override; int meander; float meander_T;
+    const glide_step_sched* sched; glide_step_sched sched0;
+    int n_steps, phys_begin, post_begin;
+    const float* noise_sub; const float* noise_mea; uint32_t seed_lo, seed_hi;
+    float* fp;
+    float fp_lon0, fp_lon_span, fp_lat0, fp_lat_span;
+    int fp_R, fp_T, fp_Z, fp_Y, fp_X;
+    const float* fp_edges;
+    float dom_lon0, dom_lon1, dom_lat0, dom_lat1, dom_alt;
+    int32_t* esc; int32_t* act;
+    uint32_t* status;
+};
+
+// ---------------------------------------------------------------------------
+// Hanna column turbulence (hanna.py:192-337, 1500-1596)
+// ---------------------------------------------------------------------------
+
+struct Surface {
+    float blh, ustar, w_star, hL, L, f_abs;
+};
+
+struct Sig6 { float su, sv, sw, tlu, tlv, tlw; };
+
+__device__ __forceinline__ Sig6 in_bl(float z, const Surface& s) {
+    Sig6 o;
+    const float blh = s.blh, us = s.ustar;
+    if (s.hL > 1.0f) {  // stable (hanna.py:192-222)
+        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
+        const float om = fmaxf(1.0f - zoh, 0.0f);
+        o.su = (2.0f * us) * om;
+        o.sw = (1.3f * us) * om;
+        o.sv = o.sw;
+        const float zf = fmaxf(zoh, 1e-6f);
+        const float sq = sqrtf(zf);
+        o.tlu = ((0.15f * blh) / fmaxf(o.su, SIGMA_MIN)) * sq;
+        o.tlv = ((0.07f * blh) / fmaxf(o.sv, SIGMA_MIN)) * sq;
+        o.tlw = ((0.10f * blh) / fmaxf(o.sw, SIGMA_MIN)) * powf(zf, 0.8f);
+    } else if (s.hL < -1.0f) {  // unstable (hanna.py:255-298)
+        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
+        const float hl = fminf(fmaxf(s.hL, -1000.0f), 0.0f);
+        o.su = powf(fmaxf(12.0f - 0.5f * hl, 1e-3f), 1.0f / 3.0f) * us;
+        o.sv = o.su;
+        const float sw2 = (((1.2f * (s.w_star * s.w_star)) * fmaxf(1.0f - 0.9f * zoh, 0.0f))
+                           * powf(zoh, 2.0f / 3.0f)) + ((1.8f - 1.4f * zoh) * (us * us));
+        o.sw = sqrtf(fmaxf(sw2, SIGMA_MIN * SIGMA_MIN));
+        o.tlu = (0.15f * blh) / fmaxf(o.su, SIGMA_MIN);
+        o.tlv = o.tlu;
+        const float azl = fmaxf(zoh * (-hl), 0.0f);
+        const float swc = fmaxf(o.sw, SIGMA_MIN);
+        if (azl < 1.0f) {
+            o.tlw = (0.1f * z) / (swc * fmaxf(0.55f - 0.38f * azl, 1e-2f));
+        } else if (zoh < 0.1f) {
+            o.tlw = (0.59f * z) / swc;
+        } else {
+            o.tlw = ((0.15f * blh) / swc) * (1.0f - expf(-5.0f * zoh));
+        }
+    } else {  // neutral (hanna.py:225-252)
+        const float fa = s.f_abs;
+        o.su = (2.0f * us) * expf(((-3.0f * fa) * z) / us);
+        o.sw = (1.3f * us) * expf(((-2.0f * fa) * z) / us);
+        o.sv = o.sw;
+        const float den = 1.0f + (((15.0f * fa) * z) / us);
+        o.tlw = ((0.5f * z) / fmaxf(o.sw, SIGMA_MIN)) / fmaxf(den, 1.0f);
+        o.tlu = o.tlw;
+        o.tlv = o.tlw;
+    }
+    return o;
+}
+
+// surface_layer_sigma_w (hanna.py:405-426)
+__device__ __forceinline__ float sl_sigma_w(float z, float us, float L) {
+    const bool finite = fabsf(L) > 1e-6f;
+    const float Ls = finite ? L : 1.0f;
+    const float zl = finite ? fminf(fmaxf(z / Ls, -50.0f), 50.0f) : 0.0f;
+    return (zl < 0.0f) ? (1.3f * us) * powf(fmaxf(1.0f - 3.0f * zl, 1e-6f), 1.0f / 3.0f) : 1.3f * us;
+}
+
+// BL profile + optional surface-layer override + FLEXPART floors, before the
+// free-troposphere override (hanna.py:1529-1565)
+__device__ __forceinline__ Sig6 bl_profile(float z, const Surface& s, int sl_override, int floors) {
+    Sig6 o = in_bl(z, s);
+    if (sl_override) {
+        const float z_sl = 0.1f * s.blh;
+        if (z < z_sl) {
+            const Sig6 c = in_bl(fmaxf(z, z_sl), s);
+            o.su = c.su;
+            o.sv = c.sv;
+            o.sw = sl_sigma_w(z, s.ustar, s.L);
+            const float zt = fmaxf(z, Z_MIN);
+            o.tlu = (KARMAN * zt) / fmaxf(o.su, SIGMA_MIN);
+            o.tlv = (KARMAN * zt) / fmaxf(o.sv, SIGMA_MIN);
+            o.tlw = (KARMAN * zt) / fmaxf(o.sw, SIGMA_MIN);
+        }
+    }
+    if (floors) {
+        o.tlu = fmaxf(o.tlu, 10.0f);
+        o.tlv = fmaxf(o.tlv, 10.0f);
+        o.tlw = fmaxf(o.tlw, 30.0f);
+    }
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// met sampling
+// ---------------------------------------------------------------------------
+
+// wind at (lon, lat, z): the RK2 wind function (hanna.py:866-889) returning
+// (dlon/dt, dlat/dt, w)
+template <typename T>
+__device__ __forceinline__ float3 wind_at(const StepDev& p, float lon, float lat, float z, float alpha) {
+    const GridDev& g = p.g;
+    const float xn = norm_h(lon, g.lon0, g.lon_span);
+    const float yn = norm_h(lat, g.lat0, g.lat_span);
+    const float zn = norm_z(z, g);
+    Tri t;
+    tri_weights(unnorm(xn, (float)(g.nx - 1)), unnorm(yn, (float)(g.ny - 1)), unnorm(zn, g.zmax_idx), g.nx, g.ny,
+                g.nz, t);
+    const T* wb = static_cast<const T*>(p.wind);
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int zz = (c & 4) ? t.z1 : t.z0;
+        const int yy = (c & 2) ? t.y1 : t.y0;
+        const int xx = (c & 1) ? t.x1 : t.x0;
+        float v[8];
+        load8(wb + cell_index(zz, yy, xx, g.ny, g.nx) * 8, v);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] = acc[k] + v[k] * t.w[c];
+    }
+    const float om = 1.0f - alpha;
+    const float u = acc[0] * om + acc[3] * alpha;
+    const float vv = acc[1] * om + acc[4] * alpha;
+    const float w = acc[2] * om + acc[5] * alpha;
+    const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
+    return make_float3(u / m_lon, vv / M_PER_DEG_LAT, w);
+}
+
+template <typename T>
+__device__ __forceinline__ void surface_at(const StepDev& p, float lon, float lat, float alpha, float out[5]) {
+    // _bilinear_at (hanna.py:1070-1085) of the lerped fields (hanna.py:805-813)
+    const GridDev& g = p.g;
+    const float xn = clamp11((2.0f * (lon - g.lon0)) / g.lon_span - 1.0f);
+    const float yn = clamp11((2.0f * (lat - g.lat0)) / g.lat_span - 1.0f);
+    const float ix = unnorm(xn, (float)(g.nx - 1));
+    const float iy = unnorm(yn, (float)(g.ny - 1));
+    const float fx = floorf(ix), fy = floorf(iy);
+    const float w = ix - fx, e = 1.0f - w, nn = iy - fy, s = 1.0f - nn;
+    const float wts[4] = {s * e, s * w, nn * e, nn * w};  // nw, ne, sw, se
+    const int xi = (int)fx, yi = (int)fy;
+    const int x0 = min(max(xi, 0), g.nx - 1), x1 = min(max(xi + 1, 0), g.nx - 1);
+    const int y0 = min(max(yi, 0), g.ny - 1), y1 = min(max(yi + 1, 0), g.ny - 1);
+    const T* sb = static_cast<const T*>(p.surf);
+    float lerped[4][5];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int yy = (c & 2) ? y1 : y0;
+        const int xx = (c & 1) ? x1 : x0;
+        const T* rec = sb + ((int64_t)yy * g.nx + xx) * 16;
+        float a[8], b[8];
+        load8(rec, a);
+        load8(rec + 8, b);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) lerped[c][f] = torch_lerp(a[f], b[f], alpha);
+    }
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        out[f] = __fmaf_rn(lerped[3][f], wts[3],
+                           __fmaf_rn(lerped[2][f], wts[2], __fmaf_rn(lerped[1][f], wts[1], lerped[0][f] * wts[0])));
+    }
+    out[1] *= Scales<T>::sp;
+}
+
+// ---------------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float noise_or_philox(const StepDev& p, const float* base, int64_t idx, float philox) {
+    return base ? __ldg(base + idx) : philox;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) step_kernel(const StepDev p) {
+    extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool have = i < p.n;
+    const int lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < 2 * p.n_steps; k += blockDim.x) s_counts[k] = 0;
+    __syncthreads();
+
+    float lon = 0.f, lat = 0.f, z = 0.f, wgt = 0.f, up = 0.f, vp = 0.f, wp = 0.f, um = 0.f, vm = 0.f;
+    float rel = 0.f, wend = 0.f;
+    int rid = 0;
+    bool alive = false;
+    if (have) {
+        lon = p.lon[i * p.ps];
+        lat = p.lat[i * p.ps];
+        z = p.z[i * p.ps];
+        wgt = p.weight[i * p.ps];
+        up = p.up[i];
+        vp = p.vp[i];
+        wp = p.wp[i];
+        if (p.meander) { um = p.um[i]; vm = p.vm[i]; }
+        rel = p.rel_off[i];
+        wend = p.win_end_off ? p.win_end_off[i] : 0.f;
+        rid = p.release_idx ? p.release_idx[i] : 0;
+        alive = p.alive ? (p.alive[i] != 0) : true;
+    }
+    const float L_sim = p.sim_length;
+    const int ms = p.max_substeps;
+    bool nonfinite = false;
+
+    for (int j = 0; j < p.n_steps; ++j) {
+        const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
+        bool active;
+        if (p.active_mask) active = have && p.active_mask[i] != 0;
+        else active = have && alive && (rel >= sc.cursor_off) && ((rel - L_sim) <= sc.cursor_off);
+
+        if (j >= p.phys_begin && active) {
+            const float delta = sc.delta, alpha = sc.alpha;
+            // --- RK2 midpoint advection, backward (hanna.py:855-896)
+            const float3 v1 = wind_at<T>(p, lon, lat, z, alpha);
+            const float hd = 0.5f * delta;
+            const float3 v2 = wind_at<T>(p, lon - hd * v1.x, lat - hd * v1.y, z - hd * v1.z, alpha);
+            lon = lon - delta * v2.x;
+            lat = lat - delta * v2.y;
+            z = z - delta * v2.z;
+
+            // --- surface fields and stability (hanna.py:950-966, 142-189)
+            float sf[5];
+            surface_at<T>(p, lon, lat, alpha, sf);
+            Surface S;
+            S.blh = fmaxf(sf[0], BLH_MIN);
+            const float sp_ = sf[1];
+            S.ustar = fmaxf(sf[2], USTAR_MIN);
+            const float shf = sf[3], ts = sf[4];
+            {
+                const float rho = sp_ / (R_DRY * ts);
+                const float denom = (float)(0.4 * GRAVITY_D) * shf;
+                const float num = -(S.ustar * S.ustar * S.ustar) * ts * rho * C_P;
+                S.L = (fabsf(denom) > 1e-10f) ? num / denom : INFINITY;
+                S.hL = S.blh / S.L;
+                const float cube = ((GRAVITY * S.blh) * shf) / ((ts * rho) * C_P);
+                S.w_star = (cube > 0.0f) ? powf(fmaxf(cube, 0.0f), 1.0f / 3.0f) : 0.0f;
+                const float f_cor = (float)(2.0 * OMEGA_D) * sinf(lat * DEG2RAD);
+                S.f_abs = fmaxf(fabsf(f_cor), 1e-5f);
+            }
+
+            // --- support brick at z_eval: FT sigma_w / T_Lw, rho, drho/dz, meander sigmas
+            const float z_ubl = p.z_ubl;
+            const float z_eval = fmaxf(z, z_ubl);
+            const GridDev& g = p.g;
+            const float ix = unnorm(norm_h(lon, g.lon0, g.lon_span), (float)(g.nx - 1));
+            const float iy = unnorm(norm_h(lat, g.lat0, g.lat_span), (float)(g.ny - 1));
+            const float iz_e = unnorm(norm_z(z_eval, g), g.zmax_idx);
+            Tri t;
+            tri_weights(ix, iy, iz_e, g.nx, g.ny, g.nz, t);
+            const T* sup = static_cast<const T*>(p.support);
+            float ftsw_c[8];
+            float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int zz = (c & 4) ? t.z1 : t.z0;
+                const int yy = (c & 2) ? t.y1 : t.y0;
+                const int xx = (c & 1) ? t.x1 : t.x0;
+                float v[8];
+                load8(sup + cell_index(zz, yy, xx, g.ny, g.nx) * 8, v);
+                ftsw_c[c] = v[0];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc[k] = acc[k] + v[k] * t.w[c];
+            }
+            const float ft_sw = acc[0], ft_tl = acc[1];
+            const float rho_p = acc[2];
+            const float drho_p = acc[3] * Scales<T>::drho;
+            const float m_su = acc[4], m_sv = acc[5];
+
+            // --- column turbulence at z_eval (hanna.py:976-982)
+            Sig6 col = bl_profile(z_eval, S, p.sl_override, p.floors);
+            if (z_eval > S.blh) {
+                col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
+                col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
+            }
+            const float su = fmaxf(col.su, SIGMA_MIN), sv = fmaxf(col.sv, SIGMA_MIN), sw = fmaxf(col.sw, SIGMA_MIN);
+            const float tlu = fmaxf(col.tlu, T_L_MIN), tlv = fmaxf(col.tlv, T_L_MIN), tlw = fmaxf(col.tlw, T_L_MIN);
+
+            // --- sigma_w at z_eval +- 1 m for the well-mixed drift (hanna.py:984-991)
+            float sw_pm[2];
+            const float z_hi = z_eval + 1.0f;
+            const float z_lo = fmaxf(z_eval - 1.0f, z_ubl);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const float zq = q == 0 ? z_hi : z_lo;
+                float s = bl_profile(zq, S, p.sl_override, p.floors).sw;
+                if (zq > S.blh) {
+                    const float izq = unnorm(norm_z(zq, g), g.zmax_idx);
+                    Tri tq;
+                    tri_weights(ix, iy, izq, g.nx, g.ny, g.nz, tq);
+                    float a = 0.f;
+                    if (tq.z0 == t.z0 && tq.z1 == t.z1) {
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) a = a + ftsw_c[c] * tq.w[c];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            const int zz = (c & 4) ? tq.z1 : tq.z0;
+                            const int yy = (c & 2) ? tq.y1 : tq.y0;
+                            const int xx = (c & 1) ? tq.x1 : tq.x0;
+                            a = a + to_f(sup[cell_index(zz, yy, xx, g.ny, g.nx) * 8]) * tq.w[c];
+                        }
+                    }
+                    s = a;
+                }
+                sw_pm[q] = fmaxf(s, SIGMA_MIN);
+            }
+            const float dsig2 = (sw_pm[0] * sw_pm[0] - sw_pm[1] * sw_pm[1]) / fmaxf(z_hi - z_lo, 1.0f);
+            const float sw_sq = fmaxf(sw * sw, SIGMA_MIN * SIGMA_MIN);
+
+            // --- density drift (hanna.py:993-1006)
+            const float rho_c = fmaxf(rho_p, 1e-3f);
+            const float drift_fwd = (sw_sq * drho_p) / rho_c;
+            const float half_bwd = -0.5f * dsig2;
+            const float dens_bwd = -drift_fwd;
+
+            // --- substep count (hanna.py:1162-1186)
+            const float kq = ceilf(delta / (p.substep_c * fmaxf(tlw, 1e-3f)));
+            int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
+            if (!(kq == kq)) k = 1;  // NaN
+            const float sub_dt = delta / (float)k;
+
+            // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
+            const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
+            const float umax = 4.0f * su, vmax = 4.0f * sv, wmax = 4.0f * sw;
+            const float au = expf(-sub_dt / tlu), av = expf(-sub_dt / tlv), aw = expf(-sub_dt / tlw);
+            const float ru = sqrtf(fmaxf(su2 * (1.0f - au * au), 0.0f));
+            const float rv = sqrtf(fmaxf(sv2 * (1.0f - av * av), 0.0f));
+            const float rw = sqrtf(fmaxf(sw2 * (1.0f - aw * aw), 0.0f));
+            const int64_t nn = p.n;
+            for (int it = 0; it < k; ++it) {
+                float eu, ev, ew;
+                if (p.noise_sub) {
+                    const float* b = p.noise_sub + ((int64_t)(j * ms + it) * 3) * nn + i;
+                    eu = __ldg(b);
+                    ev = __ldg(b + nn);
+                    ew = __ldg(b + 2 * nn);
+                } else {
+                    const U4 r = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sc.step_index,
+                                                  STREAM_SUBSTEP + (uint32_t)it}, p.seed_lo, p.seed_hi);
+                    const float2 n01 = box_muller(r.x, r.y);
+                    const float2 n23 = box_muller(r.z, r.w);
+                    eu = n01.x; ev = n01.y; ew = n23.x;
+                }
+                const float factor = 1.0f + (wp * wp) / sw_sq;
+                const float drift_w = factor * half_bwd + dens_bwd;
+                float un = (au * up + 0.0f * sub_dt) + ru * eu;
+                float vn = (av * vp + 0.0f * sub_dt) + rv * ev;
+                float wn = (aw * wp + drift_w * sub_dt) + rw * ew;
+                wn = fminf(fmaxf(wn, -wmax), wmax);
+                un = fminf(fmaxf(un, -umax), umax);
+                vn = fminf(fmaxf(vn, -vmax), vmax);
+                z = z + (-wn) * sub_dt;
+                const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
+                lon = lon + ((-un) * sub_dt) / m_lon;
+                lat = lat + ((-vn) * sub_dt) / M_PER_DEG_LAT;
+                if (z < 0.0f) {
+                    z = 0.0f - z;
+                    wn = -wn;
+                }
+                up = un; vp = vn; wp = wn;
+            }
+
+            // --- meander (hanna.py:1028-1054)
+            if (p.meander) {
+                float e0, e1;
+                if (p.noise_mea) {
+                    const float* b = p.noise_mea + ((int64_t)j * 2) * nn + i;
+                    e0 = __ldg(b);
+                    e1 = __ldg(b + nn);
+                } else {
+                    const U4 r = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sc.step_index,
+                                                  STREAM_MEANDER}, p.seed_lo, p.seed_hi);
+                    const float2 n01 = box_muller(r.x, r.y);
+                    e0 = n01.x; e1 = n01.y;
+                }
+                const float am = expf(-delta / p.meander_T);
+                const float one_m = 1.0f - am * am;
+                const float umn = (am * um + 0.0f * delta) + sqrtf(fmaxf((m_su * m_su) * one_m, 0.0f)) * e0;
+                const float vmn = (am * vm + 0.0f * delta) + sqrtf(fmaxf((m_sv * m_sv) * one_m, 0.0f)) * e1;
+                const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
+                lon = lon + ((-umn) * delta) / m_lon;
+                lat = lat + ((-vmn) * delta) / M_PER_DEG_LAT;
+                um = umn; vm = vmn;
+            }
+            nonfinite |= !(isfinite(lon) && isfinite(lat) && isfinite(z) && isfinite(up) && isfinite(vp) &&
+                           isfinite(wp));
+        }
+
+        if (j >= p.post_begin) {
+            // --- time-ago bin (main.py:1459-1465) and footprint (footprint_gridder.py:154-197)
+            bool valid = false;
+            int64_t flat = -1;
+            if (active && p.fp) {
+                const float el = fmaxf(wend - sc.cursor_off, 0.0f);
+                int tb = (int)floorf(el / 3600.0f);
+                if (p.fp_T == 1) tb = min(tb, 0);
+                const float xf = floorf(((lon - p.fp_lon0) / p.fp_lon_span) * (float)p.fp_X);
+                const float yf = floorf(((lat - p.fp_lat0) / p.fp_lat_span) * (float)p.fp_Y);
+                int zb = 0;
+                for (int e = 0; e <= p.fp_Z; ++e) zb += (__ldg(p.fp_edges + e) < z) ? 1 : 0;
+                zb -= 1;
+                valid = (rid >= 0) && (rid < p.fp_R) && (xf >= 0.0f) && (xf < (float)p.fp_X) && (yf >= 0.0f) &&
+                        (yf < (float)p.fp_Y) && (zb >= 0) && (zb < p.fp_Z) && (tb >= 0) && (tb < p.fp_T);
+                if (valid) {
+                    flat = ((((int64_t)rid * p.fp_T + tb) * p.fp_Z + zb) * p.fp_Y + (int64_t)yf) * p.fp_X + (int64_t)xf;
+                }
+            }
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                // warp-aggregated atomic: lanes hitting the same cell sum by shuffles, one atomic per cell
+                const float w_eff = wgt * sc.delta;
+                const unsigned peers = __match_any_sync(vmask, (unsigned long long)flat);
+                float sum = 0.0f;
+                unsigned m = peers;
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    sum += __shfl_sync(peers, w_eff, src);
+                }
+                if (lane == __ffs(peers) - 1) atomicAdd(p.fp + flat, sum);
+            }
+            // --- escape kill (main.py:690-711, 1475-1477)
+            bool escaped = false;
+            if (active) {
+                const bool within = (lon >= p.dom_lon0) && (lon <= p.dom_lon1) && (lat >= p.dom_lat0) &&
+                                    (lat <= p.dom_lat1) && (z <= p.dom_alt);
+                escaped = !within;
+                if (escaped) alive = false;
+            }
+            const int n_esc = __popc(__ballot_sync(0xffffffffu, escaped));
+            const int n_act = __popc(__ballot_sync(0xffffffffu, active));
+            if (lane == 0) {
+                if (n_esc) atomicAdd(&s_counts[j], n_esc);
+                if (n_act) atomicAdd(&s_counts[p.n_steps + j], n_act);
+            }
+        }
+    }
+
+    if (have) {
+        p.lon[i * p.ps] = lon;
+        p.lat[i * p.ps] = lat;
+        p.z[i * p.ps] = z;
+        p.up[i] = up;
+        p.vp[i] = vp;
+        p.wp[i] = wp;
+        if (p.meander) { p.um[i] = um; p.vm[i] = vm; }
+        if (p.alive) p.alive[i] = alive ? 1 : 0;
+        if (nonfinite && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_NONFINITE_STATE);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < p.n_steps; k += blockDim.x) {
+        if (p.esc && s_counts[k]) atomicAdd(p.esc + k, s_counts[k]);
+        if (p.act && s_counts[p.n_steps + k]) atomicAdd(p.act + k, s_counts[p.n_steps + k]);
+    }
+}
+
+template <typename T>
+static glide_status launch_step(const StepDev& d, cudaStream_t stream) {
+    const int threads = 128;
+    const int64_t blocks = (d.n + threads - 1) / threads;
+    const size_t smem = sizeof(int32_t) * 2 * (size_t)d.n_steps;
+    if (smem > 48 * 1024) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large", d.n_steps);
+    step_kernel<T><<<(unsigned)blocks, threads, smem, stream>>>(d);
+    return check_launch("glide_step");
+}
+
+}  // namespace glide
+
+using namespace glide;
+
+extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
+    if (!a) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: args is NULL");
+    if (a->n < 0) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n < 0");
+    if (a->n_steps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps < 1");
+    if (!a->sched && a->n_steps != 1)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: sched is NULL but n_steps = %d", a->n_steps);
+    if (a->n == 0) return GLIDE_OK;
+    if (!a->lon || !a->lat || !a->z || !a->weight || !a->u_prime || !a->v_prime || !a->w_prime || !a->rel_off)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: a particle state pointer is NULL");
+    if (a->meander_enabled && (!a->u_meander || !a->v_meander || !a->support_packed))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: meander enabled but meander state is NULL");
+    if (!a->wind_packed || !a->surf_packed || !a->support_packed || !a->grid.level_sorted)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: packed met pointer is NULL");
+    if (a->grid.nz < 2 || a->grid.ny < 2 || a->grid.nx < 2)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: grid must be at least 2x2x2");
+    if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
+    if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
+    if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
+                         a->fp.n_time_bins < 1 || a->fp.n_releases < 1))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: invalid footprint grid");
+    if (a->post_begin < a->n_steps && !a->active_mask && a->footprint && !a->win_end_off)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: footprint needs win_end_off");
+    if (a->grid.lon_last == a->grid.lon_first || a->grid.lat_last == a->grid.lat_first)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: met grid has zero span");
+    if (((uintptr_t)a->wind_packed | (uintptr_t)a->surf_packed | (uintptr_t)a->support_packed) & 15u)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: packed met must be 16-byte aligned");
+
+    StepDev d;
+    d.n = a->n;
+    d.lon = a->lon; d.lat = a->lat; d.z = a->z; d.weight = a->weight; d.ps = a->pos_stride;
+    d.up = a->u_prime; d.vp = a->v_prime; d.wp = a->w_prime; d.um = a->u_meander; d.vm = a->v_meander;
+    d.rel_off = a->rel_off; d.win_end_off = a->win_end_off; d.release_idx = a->release_idx;
+    d.alive = a->alive; d.active_mask = a->active_mask;
+    d.sim_length = a->sim_length_s;
+    d.wind = a->wind_packed; d.surf = a->surf_packed; d.support = a->support_packed;
+    d.g = make_grid_dev(a->grid);
+    d.substep_c = a->substep_c; d.max_substeps = a->max_substeps; d.z_ubl = a->z_ubl_m;
+    d.floors = a->flexpart_tl_floors; d.sl_override = a->surface_layer_override;
+    d.meander = a->meander_enabled; d.meander_T = a->meander_timescale_s;
+    d.sched = a->sched; d.sched0 = a->sched0;
+    d.n_steps = a->n_steps; d.phys_begin = a->phys_begin; d.post_begin = a->post_begin;
+    d.noise_sub = a->noise_substep; d.noise_mea = a->noise_meander;
+    d.seed_lo = (uint32_t)a->seed; d.seed_hi = (uint32_t)(a->seed >> 32);
+    d.fp = a->footprint;
+    d.fp_lon0 = (float)a->fp.lon_min;
+    d.fp_lon_span = (float)fmax(1e-6, a->fp.lon_max - a->fp.lon_min);
+    d.fp_lat0 = (float)a->fp.lat_min;
+    d.fp_lat_span = (float)fmax(1e-6, a->fp.lat_max - a->fp.lat_min);
+    d.fp_R = a->fp.n_releases; d.fp_T = a->fp.n_time_bins; d.fp_Z = a->fp.n_z; d.fp_Y = a->fp.n_y;
+    d.fp_X = a->fp.n_x; d.fp_edges = a->fp.z_edges;
+    d.dom_lon0 = (float)a->dom_lon_min; d.dom_lon1 = (float)a->dom_lon_max;
+    d.dom_lat0 = (float)a->dom_lat_min; d.dom_lat1 = (float)a->dom_lat_max;
+    d.dom_alt = (float)a->dom_alt_max;
+    d.esc = a->escaped_per_step; d.act = a->active_per_step;
+    d.status = a->status;
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a->met_dtype) {
+        case GLIDE_MET_F32: return launch_step<float>(d, s);
+        case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s);
+        case GLIDE_MET_F16: return launch_step<__half>(d, s);
+        default: return set_error(GLIDE_ERR_UNSUPPORTED, "glide_step: unknown met_dtype %d", a->met_dtype);
+    }
+}

@@ -1,0 +1,366 @@
+"""Fused batch runtime: the reference's per-step cursor loop, one met window per launch.
+
+Replaces the static branch of the reference's cursor loop
+(``src/lpdm/main.py:1382-1477``: active mask, met window and RK2 weight, the
+scheme step, once-per-window convection, time-ago bin, footprint scatter-add,
+escape kill) for one batch. The host computes the step schedule exactly as the
+reference does (cursor arithmetic in ``datetime``, float32 rounding of the
+cursor offset) and then issues, per met window,
+
+* without convection: ONE ``glide_step`` launch covering every outer step of
+  the window (physics + footprint + escape fused, state in registers);
+* with convection: ``glide_step`` for the physics of the window's first step,
+  ``glide_convect`` (column build + redistribution on the device), then one
+  ``glide_step`` that does the first step's footprint/escape and all remaining
+  steps — the reference's step -> convection -> footprint -> kill order.
+
+No launch synchronises with the host; per-step diagnostics (escaped and
+active counts) accumulate in device arrays read once per batch.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from collections.abc import Callable
+from dataclasses import dataclass, field
+from datetime import UTC, datetime, timedelta
+
+import numpy as np
+import torch
+
+from glide_b200 import _abi
+from glide_b200.window import GridInfo, PackedWindow, WindowFields, stream_handle
+
+
+@dataclass(frozen=True)
+class HannaConfig:
+    """``HannaScheme`` knobs (src/lpdm/turbulence/hanna.py:440-520)."""
+
+    meander_enabled: bool = False
+    meander_coefficient: float = 0.16
+    meander_stencil_radius: int = 1
+    meander_timescale_seconds: float = 1800.0
+    substep_c: float = 0.5
+    max_substeps: int = 50
+    z_ubl_m: float = 2.0
+    flexpart_tl_floors: bool = True
+    surface_layer_override: bool = False
+
+
+@dataclass(frozen=True)
+class EmanuelConfig:
+    """``EmanuelReducedConvection`` knobs (src/lpdm/convection/emanuel.py:531-565)."""
+
+    closure_c: float = 0.03
+    trigger_dtv_k: float = 0.9
+    min_cape_j_kg: float = 50.0
+    min_cloud_depth_m: float = 500.0
+
+
+@dataclass(frozen=True)
+class FootprintSpec:
+    """``OutputGridConfig`` and the gridder's release count (src/lpdm/config.py:360-382)."""
+
+    lon_bounds: tuple[float, float]
+    lat_bounds: tuple[float, float]
+    n_x: int
+    n_y: int
+    z_edges: tuple[float, ...]
+    n_time_bins: int
+    n_releases: int = 1
+
+    @property
+    def shape(self) -> tuple[int, int, int, int, int]:
+        return (self.n_releases, self.n_time_bins, len(self.z_edges) - 1, self.n_y, self.n_x)
+
+
+@dataclass(frozen=True)
+class DomainSpec:
+    """``MetDomainConfig`` bounds of the escape kill (src/lpdm/main.py:690-711)."""
+
+    lon_bounds: tuple[float, float]
+    lat_bounds: tuple[float, float]
+    alt_max_m: float
+
+
+@dataclass
+class ParticleState:
+    """Structure-of-arrays particle state on the device."""
+
+    lon: torch.Tensor
+    lat: torch.Tensor
+    z: torch.Tensor
+    weight: torch.Tensor
+    u_prime: torch.Tensor
+    v_prime: torch.Tensor
+    w_prime: torch.Tensor
+    u_meander: torch.Tensor
+    v_meander: torch.Tensor
+    rel_off: torch.Tensor
+    win_end_off: torch.Tensor
+    release_idx: torch.Tensor  # int32
+    alive: torch.Tensor  # uint8
+
+    @property
+    def n(self) -> int:
+        return self.lon.numel()
+
+    @classmethod
+    def from_particles(cls, particles, rel_off, win_end_off, release_idx, device) -> ParticleState:
+        """From the reference's ``(N, 4)`` [lon, lat, z, weight] layout and sidecars
+        (``ParticleBatch``, src/lpdm/release_generator.py:202-237)."""
+        p = torch.as_tensor(particles, dtype=torch.float32)
+        if p.dim() != 2 or p.shape[1] != 4:
+            raise ValueError("particles must have shape (N, 4)")
+        n = p.shape[0]
+        p = p.to(device)
+        z = torch.zeros(n, dtype=torch.float32, device=device)
+        return cls(p[:, 0].contiguous(), p[:, 1].contiguous(), p[:, 2].contiguous(), p[:, 3].contiguous(),
+                   z.clone(), z.clone(), z.clone(), z.clone(), z.clone(),
+                   torch.as_tensor(rel_off, dtype=torch.float32).to(device),
+                   torch.as_tensor(win_end_off, dtype=torch.float32).to(device),
+                   torch.as_tensor(release_idx).to(device=device, dtype=torch.int32),
+                   torch.ones(n, dtype=torch.uint8, device=device))
+
+    def particles(self) -> torch.Tensor:
+        return torch.stack([self.lon, self.lat, self.z, self.weight], dim=1)
+
+
+@dataclass
+class StepPlan:
+    cursor: datetime
+    cursor_off: float
+    delta: float
+    hour: datetime
+    alpha: float = 0.0
+
+
+def hour_floor(t: datetime) -> datetime:
+    """main.py:380-381"""
+    return t.astimezone(UTC).replace(minute=0, second=0, microsecond=0)
+
+
+def plan_steps(batch_start: datetime, cursor_start: datetime, cursor_terminus: datetime,
+               dt_seconds: float) -> list[StepPlan]:
+    """The cursor walk of main.py:1383-1389, 1610 with the alpha of main.py:916-919
+    for hourly windows [hour, hour + 1 h]."""
+    steps = []
+    t = cursor_start
+    b = batch_start.timestamp()
+    while t > cursor_terminus:
+        delta = min(float(dt_seconds), (t - cursor_terminus).total_seconds())
+        hk = hour_floor(t)
+        ts, te = hk.timestamp(), (hk + timedelta(hours=1)).timestamp()
+        alpha = max(0.0, min(1.0, (t.timestamp() - 0.5 * delta - ts) / max(1.0, te - ts)))
+        steps.append(StepPlan(t, t.timestamp() - b, delta, hk, alpha))
+        t = t - timedelta(seconds=delta)
+    return steps
+
+
+def schedule_array(steps: list[StepPlan]) -> np.ndarray:
+    """``glide_step_sched`` records (float32 cursor offset, delta, alpha; int32 index)."""
+    rec = np.zeros(len(steps), dtype=np.dtype([("c", "<f4"), ("d", "<f4"), ("a", "<f4"), ("i", "<i4")]))
+    for k, s in enumerate(steps):
+        rec[k] = (np.float32(s.cursor_off), np.float32(s.delta), np.float32(s.alpha), k)
+    return rec
+
+
+@dataclass
+class BatchOutput:
+    state: ParticleState
+    footprint: torch.Tensor
+    escaped_per_step: np.ndarray
+    active_per_step: np.ndarray
+    n_steps: int
+    convection: list = field(default_factory=list)  # (window start, n_moved device tensor)
+    status: int = 0
+
+
+class BatchRun:
+    """One batch in flight. ``step_window()`` issues the launches of the next window."""
+
+    def __init__(self, runner: BatchRunner, state: ParticleState, steps: list[StepPlan], sim_length_s: float) -> None:
+        self.r = runner
+        self.state = state
+        self.steps = steps
+        self.sim_length_s = float(sim_length_s)
+        dev = runner.device
+        self.sched_dev = torch.from_numpy(schedule_array(steps).view(np.uint8).copy()).to(dev)
+        self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
+        self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.footprint = torch.zeros(runner.footprint.shape, dtype=torch.float32, device=dev)
+        self.z_edges = torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32), device=dev)
+        # windows = runs of consecutive steps with the same hour
+        self.windows: list[tuple[int, int]] = []
+        k = 0
+        while k < len(steps):
+            e = k
+            while e < len(steps) and steps[e].hour == steps[k].hour:
+                e += 1
+            self.windows.append((k, e))
+            k = e
+        self.next_window = 0
+        self.conv_log: list = []
+        self.conv_scratch = None
+
+    @property
+    def done(self) -> bool:
+        return self.next_window >= len(self.windows)
+
+    def _step_args(self, packed: PackedWindow, j0: int, n_steps: int, phys_begin: int, post_begin: int,
+                   noise) -> _abi.StepArgs:
+        r, s = self.r, self.state
+        h = r.hanna
+        a = _abi.StepArgs()
+        a.n = s.n
+        a.lon, a.lat, a.z, a.weight = s.lon.data_ptr(), s.lat.data_ptr(), s.z.data_ptr(), s.weight.data_ptr()
+        a.pos_stride = 1
+        a.u_prime, a.v_prime, a.w_prime = s.u_prime.data_ptr(), s.v_prime.data_ptr(), s.w_prime.data_ptr()
+        a.u_meander, a.v_meander = s.u_meander.data_ptr(), s.v_meander.data_ptr()
+        a.rel_off, a.win_end_off = s.rel_off.data_ptr(), s.win_end_off.data_ptr()
+        a.release_idx, a.alive, a.active_mask = s.release_idx.data_ptr(), s.alive.data_ptr(), None
+        a.sim_length_s = self.sim_length_s
+        a.wind_packed, a.surf_packed, a.support_packed = (packed.wind.data_ptr(), packed.surf.data_ptr(),
+                                                          packed.support.data_ptr())
+        a.met_dtype = packed.code
+        a.grid = r.grid.c_grid()
+        a.substep_c, a.max_substeps, a.z_ubl_m = h.substep_c, h.max_substeps, h.z_ubl_m
+        a.flexpart_tl_floors, a.surface_layer_override = int(h.flexpart_tl_floors), int(h.surface_layer_override)
+        a.meander_enabled, a.meander_timescale_s = int(h.meander_enabled), h.meander_timescale_seconds
+        a.sched = self.sched_dev.data_ptr() + 16 * j0
+        a.n_steps, a.phys_begin, a.post_begin = n_steps, phys_begin, post_begin
+        if noise is not None:
+            sub, mea = noise
+            a.noise_substep = sub.data_ptr()
+            a.noise_meander = None if mea is None else mea.data_ptr()
+        a.seed = r.seed
+        a.footprint = self.footprint.data_ptr()
+        fp = r.footprint
+        a.fp = _abi.FootprintGrid(fp.lon_bounds[0], fp.lon_bounds[1], fp.lat_bounds[0], fp.lat_bounds[1],
+                                  fp.n_releases, fp.n_time_bins, len(fp.z_edges) - 1, fp.n_y, fp.n_x,
+                                  self.z_edges.data_ptr())
+        d = r.domain
+        a.dom_lon_min, a.dom_lon_max = d.lon_bounds
+        a.dom_lat_min, a.dom_lat_max = d.lat_bounds
+        a.dom_alt_max = d.alt_max_m
+        a.escaped_per_step = self.esc.data_ptr() + 4 * j0
+        a.active_per_step = self.act.data_ptr() + 4 * j0
+        a.status = self.status.data_ptr()
+        return a
+
+    def step_window(self, stream=None) -> bool:
+        """Issue the launches of the next met window; False when the batch is done."""
+        if self.done:
+            return False
+        r = self.r
+        j0, j1 = self.windows[self.next_window]
+        self.next_window += 1
+        first = self.steps[j0]
+        wf = r.window_provider(first.hour)
+        if wf.time_start != first.hour:
+            raise ValueError(f"window provider returned {wf.time_start} for hour {first.hour}")
+        packed = r.packed_for(wf, stream)
+        noise = r.noise_provider(list(range(j0, j1))) if r.noise_provider is not None else None
+        sh = stream_handle(stream)
+        n = j1 - j0
+        if r.emanuel is not None:
+            a = self._step_args(packed, j0, 1, 0, 1, noise)
+            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+            self._convect(wf, j0, stream)
+            a = self._step_args(packed, j0, n, 1, 0, noise)
+            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+        else:
+            a = self._step_args(packed, j0, n, 0, 0, noise)
+            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+        return True
+
+    def _convect(self, wf: WindowFields, j: int, stream) -> None:
+        r, s, e = self.r, self.state, self.r.emanuel
+        nz, ny, nx = r.grid.shape
+        if self.conv_scratch is None:
+            nb = C.c_size_t()
+            _abi.check(_abi.lib.glide_convect_scratch_bytes(nz, C.byref(nb)), "glide_convect_scratch_bytes")
+            self.conv_scratch = torch.zeros(nb.value // 8, dtype=torch.float64, device=r.device)
+        moved = torch.zeros(1, dtype=torch.int32, device=r.device)
+        st = self.steps[j]
+        a = _abi.ConvectArgs()
+        a.n = s.n
+        a.z, a.z_stride = s.z.data_ptr(), 1
+        a.rel_off, a.alive, a.active_mask = s.rel_off.data_ptr(), s.alive.data_ptr(), None
+        a.sim_length_s = self.sim_length_s
+        a.sched = _abi.StepSched(np.float32(st.cursor_off), st.delta, st.alpha, j)
+        a.nz, a.ny, a.nx = nz, ny, nx
+        for k, snap in enumerate((wf.start, wf.end)):
+            a.t[k] = snap["t"].data_ptr()
+            a.q[k] = snap["q"].data_ptr()
+        a.height3d = None if wf.height3d is None else wf.height3d.data_ptr()
+        a.height_level = r.grid.height_level_dev.data_ptr()
+        a.pressure_hpa = r.grid.p_hpa_dev.data_ptr()
+        a.alpha = st.alpha
+        a.closure_c, a.trigger_dtv_k = e.closure_c, e.trigger_dtv_k
+        a.min_cape_j_kg, a.min_cloud_depth_m = e.min_cape_j_kg, e.min_cloud_depth_m
+        u = r.conv_uniform_provider(j) if r.conv_uniform_provider is not None else None
+        a.uniforms = None if u is None else u.data_ptr()
+        a.seed = r.seed
+        a.scratch = self.conv_scratch.data_ptr()
+        a.n_moved = moved.data_ptr()
+        _abi.check(_abi.lib.glide_convect(C.byref(a), stream_handle(stream)), "glide_convect")
+        self.conv_log.append((wf.time_start, moved))
+
+    def run(self, stream=None) -> BatchOutput:
+        while self.step_window(stream):
+            pass
+        return self.finish()
+
+    def finish(self) -> BatchOutput:
+        n = len(self.steps)
+        status = int(self.status.item())
+        return BatchOutput(self.state, self.footprint, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
+                           self.conv_log, status)
+
+
+class BatchRunner:
+    """Runs batches of particles backward through hourly met windows on one GPU.
+
+    ``window_provider(hour)`` returns the ``[hour, hour + 1 h]`` window as device
+    ``WindowFields`` (for example ``SyntheticMet``'s fields, or
+    ``window_from_hourly`` of a reader's ``HourlyMetTensors``). ``noise_provider``
+    (parity runs) returns injected normals for a list of step indices; without
+    it the kernels draw Philox-4x32-10 normals keyed by ``seed``.
+    """
+
+    def __init__(self, *, grid: GridInfo, window_provider: Callable[[datetime], WindowFields], hanna: HannaConfig,
+                 footprint: FootprintSpec, domain: DomainSpec, emanuel: EmanuelConfig | None = None,
+                 met_dtype: str = "f32", device="cuda", seed: int = 0,
+                 noise_provider: Callable | None = None, conv_uniform_provider: Callable | None = None) -> None:
+        self.device = torch.device(device)
+        self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
+        self.window_provider = window_provider
+        self.hanna = hanna
+        self.footprint = footprint
+        self.domain = domain
+        self.emanuel = emanuel
+        self.met_dtype = met_dtype
+        self.seed = int(seed)
+        self.noise_provider = noise_provider
+        self.conv_uniform_provider = conv_uniform_provider
+        self._packed = PackedWindow(self.grid, met_dtype, self.device)
+
+    def packed_for(self, wf: WindowFields, stream=None) -> PackedWindow:
+        if self._packed.key != wf.time_start:
+            self._packed.pack(wf, meander_coefficient=self.hanna.meander_coefficient,
+                              meander_radius=self.hanna.meander_stencil_radius,
+                              build_meander=self.hanna.meander_enabled, stream=stream)
+        return self._packed
+
+    def start(self, state: ParticleState, *, batch_start: datetime, cursor_start: datetime,
+              cursor_terminus: datetime, sim_length_s: float, dt_seconds: float,
+              max_steps: int | None = None) -> BatchRun:
+        steps = plan_steps(batch_start, cursor_start, cursor_terminus, dt_seconds)
+        if max_steps is not None:
+            steps = steps[:max_steps]
+        return BatchRun(self, state, steps, sim_length_s)
+
+    def run(self, state: ParticleState, **kw) -> BatchOutput:
+        return self.start(state, **kw).run()

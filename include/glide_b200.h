@@ -1,0 +1,208 @@
+/*
+ * glide_b200 — C ABI of the B200 particle-step engine for GLIDE (mrghg/glide).
+ *
+ * Plain C: device pointers, sizes and a cudaStream_t passed as void*. No torch
+ * types. Every entry point returns a glide_status (0 = ok); the text of the
+ * last error on the calling thread is available from glide_last_error().
+ * Launches are asynchronous on the given stream and perform no host
+ * synchronisation, so they can be captured in a CUDA graph.
+ *
+ * Each entry point below names the reference interface it replaces
+ * (file:line within the reference project).
+ */
+#ifndef GLIDE_B200_H
+#define GLIDE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t glide_status;
+enum {
+    GLIDE_OK = 0,
+    GLIDE_ERR_INVALID_ARG = 1,
+    GLIDE_ERR_CUDA = 2,
+    GLIDE_ERR_UNSUPPORTED = 3,
+};
+
+/* storage type of the packed met bricks */
+enum { GLIDE_MET_F32 = 0, GLIDE_MET_BF16 = 1, GLIDE_MET_F16 = 2 };
+
+/* bits of the device status word (glide_step_args.status) */
+enum {
+    GLIDE_STATUS_NONFINITE_STATE = 1u << 0, /* a particle's state became NaN/inf */
+};
+
+/* Met grid geometry: GridInterpolationBounds (src/lpdm/gpu_engine.py:100-121). */
+typedef struct glide_grid {
+    int32_t nz, ny, nx;
+    int32_t ascending;           /* 1 if level[0] < level[nz-1] in the grid's own order */
+    double lon_first, lon_last;  /* cell-centre coordinates of x = 0 and x = nx-1 */
+    double lat_first, lat_last;  /* cell-centre coordinates of y = 0 and y = ny-1 */
+    const float* level_sorted;   /* device [nz], AGL heights sorted ascending */
+} glide_grid;
+
+/*
+ * One met window [time_start, time_end]: raw fields of the two snapshots
+ * (index 0 = start, 1 = end) as device float32 arrays. 3-D fields are
+ * [nz][ny][nx] C-contiguous in the grid's level order; 2-D fields [ny][nx].
+ */
+typedef struct glide_window_desc {
+    glide_grid grid;
+    const float* u[2];
+    const float* v[2];
+    const float* w[2];
+    const float* t[2];           /* 3-D temperature */
+    const float* t_lowest[2];    /* [ny][nx] temperature at the lowest level */
+    const float* blh[2];
+    const float* sp[2];
+    const float* ustar[2];
+    const float* shf[2];
+    const float* height3d;       /* [nz][ny][nx] AGL heights, or NULL ... */
+    const float* height_level;   /* ... then [nz] per-level heights broadcast over columns */
+    const float* pressure_hpa;   /* device [nz] bbox-mean pressure per level */
+    float meander_coefficient;
+    int32_t meander_radius;
+    int32_t build_meander;
+    int32_t met_dtype;           /* GLIDE_MET_* of the packed outputs */
+    /* outputs (caller-allocated, sizes from glide_window_packed_bytes) */
+    void* wind_packed;           /* [nz][ny][nx][8]: u0 v0 w0 u1 v1 w1 - - */
+    void* surf_packed;           /* [ny][nx][16]: blh sp ustar shf t - - - (start), same (end) */
+    void* support_packed;        /* [nz][ny][nx][8]: ft_sigma_w ft_T_Lw rho drho/dz meander_su meander_sv - - */
+} glide_window_desc;
+
+/* Per-outer-step schedule entry, computed on the host exactly as the
+ * reference runtime does (src/lpdm/main.py:1386-1420, 892-919). */
+typedef struct glide_step_sched {
+    float cursor_off;  /* float32(cursor time - batch start), seconds */
+    float delta;       /* outer step length, seconds */
+    float alpha;       /* RK2 midpoint time weight in [0, 1] */
+    int32_t step_index;/* global step number (Philox counter / noise row) */
+} glide_step_sched;
+
+/* Output grid of FootprintGridder (src/lpdm/footprint_gridder.py:50-115). */
+typedef struct glide_footprint_grid {
+    double lon_min, lon_max, lat_min, lat_max;
+    int32_t n_releases, n_time_bins, n_z, n_y, n_x;
+    const float* z_edges;        /* device [n_z + 1], ascending */
+} glide_footprint_grid;
+
+typedef struct glide_step_args {
+    int64_t n;                    /* particles */
+    /* particle state (device, float32). Position fields share pos_stride:
+     * 1 for structure-of-arrays, 4 for the reference's (N, 4) [lon, lat, z, weight]. */
+    float* lon; float* lat; float* z; float* weight; int64_t pos_stride;
+    float* u_prime; float* v_prime; float* w_prime;
+    float* u_meander; float* v_meander;      /* NULL when meander is off */
+    const float* rel_off;                    /* release time offsets (s after batch start) */
+    const float* win_end_off;                /* release window end offsets */
+    const int32_t* release_idx;              /* batch-local release index */
+    uint8_t* alive;                          /* liveness (updated by the escape kill) */
+    const uint8_t* active_mask;              /* if non-NULL, overrides the computed active mask */
+    float sim_length_s;
+    /* packed window (glide_window_pack) */
+    const void* wind_packed; const void* surf_packed; const void* support_packed;
+    int32_t met_dtype;
+    glide_grid grid;
+    /* HannaScheme parameters (src/lpdm/turbulence/hanna.py:440-520) */
+    float substep_c; int32_t max_substeps; float z_ubl_m;
+    int32_t flexpart_tl_floors; int32_t surface_layer_override;
+    int32_t meander_enabled; float meander_timescale_s;
+    /* steps of this launch: sched[0 .. n_steps) (device), or sched0 when sched == NULL and n_steps == 1.
+     * Physics runs for steps j >= phys_begin, the footprint+escape post-step for j >= post_begin. */
+    const glide_step_sched* sched; glide_step_sched sched0;
+    int32_t n_steps; int32_t phys_begin; int32_t post_begin;
+    /* noise: injected standard normals noise_substep[j][max_substeps][3][n] and
+     * noise_meander[j][2][n] (j = step within this launch), or, when NULL,
+     * Philox-4x32-10 draws keyed by seed and counted by (particle, step_index). */
+    const float* noise_substep; const float* noise_meander; uint64_t seed;
+    /* post-step (footprint + escape kill) */
+    float* footprint;                        /* [R][T][Zb][Y][X], may be NULL (no accumulation) */
+    glide_footprint_grid fp;
+    double dom_lon_min, dom_lon_max, dom_lat_min, dom_lat_max, dom_alt_max;
+    int32_t* escaped_per_step;               /* [n_steps] counters (added to), may be NULL */
+    int32_t* active_per_step;                /* [n_steps] counters (added to), may be NULL */
+    uint32_t* status;                        /* device status word (GLIDE_STATUS_*), may be NULL */
+} glide_step_args;
+
+/* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */
+typedef struct glide_convect_args {
+    int64_t n;
+    float* z; int64_t z_stride;              /* particle heights (updated) */
+    const float* rel_off; const uint8_t* alive; const uint8_t* active_mask;
+    float sim_length_s;
+    glide_step_sched sched;                  /* the first step of the window */
+    int32_t nz, ny, nx;
+    const float* t[2]; const float* q[2];    /* [nz][ny][nx] snapshots */
+    const float* height3d; const float* height_level;
+    const float* pressure_hpa;               /* [nz] */
+    float alpha;
+    float closure_c, trigger_dtv_k, min_cape_j_kg, min_cloud_depth_m;
+    const float* uniforms;                   /* injected [2][n] uniforms, or NULL → Philox(seed) */
+    uint64_t seed;
+    void* scratch;                           /* glide_convect_scratch_bytes(nz) bytes, device */
+    int32_t* n_moved;                        /* device counter (added to), may be NULL */
+} glide_convect_args;
+
+/* --- library ------------------------------------------------------------------ */
+
+/* Version of this ABI (major * 10000 + minor * 100 + patch). */
+int32_t glide_version(void);
+
+/* Copies the last error message of the calling thread into buf (NUL-terminated). */
+glide_status glide_last_error(char* buf, size_t len);
+
+/* sizeof of the ABI structs, in declaration order: glide_grid, glide_window_desc,
+ * glide_step_sched, glide_footprint_grid, glide_step_args, glide_convect_args.
+ * Lets a binding verify its struct layouts. Writes min(n, 6) values. */
+glide_status glide_abi_struct_sizes(size_t* out, int32_t n);
+
+/* --- per-window met packing ------------------------------------------------------
+ * Replaces the per-window device staging and support-field builds of
+ * HannaScheme: _cached_raw_device_met (src/lpdm/turbulence/hanna.py:747-796),
+ * _free_trop_fields (:1694-1745), _density_fields (:1747-1784) and
+ * _meander_sigma_fields (:1786-1830). */
+glide_status glide_window_packed_bytes(int32_t nz, int32_t ny, int32_t nx, int32_t met_dtype,
+                                       size_t* wind_bytes, size_t* surf_bytes, size_t* support_bytes);
+glide_status glide_window_pack(const glide_window_desc* desc, void* stream);
+
+/* --- the fused particle step ---------------------------------------------------
+ * One launch runs n_steps outer steps of the static step body for every
+ * particle: HannaScheme._step_core (src/lpdm/turbulence/hanna.py:898-1068,
+ * with _advect_rk2 :855-896 and _integrate_vertical_substeps_static
+ * :1224-1368), and after each step the runtime's footprint scatter-add
+ * (FootprintGridder.accumulate, src/lpdm/footprint_gridder.py:117-197) and
+ * escape kill (src/lpdm/main.py:1459-1477, 690-711). */
+glide_status glide_step(const glide_step_args* args, void* stream);
+
+/* --- footprint accumulation alone -----------------------------------------------
+ * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the
+ * per-step plug-in path. t_idx and release_idx are int32 [n]; positions follow
+ * pos_stride as in glide_step_args. */
+glide_status glide_footprint_accumulate(int64_t n, const float* lon, const float* lat, const float* z,
+                                        int64_t pos_stride, const uint8_t* active, const float* weights,
+                                        int64_t weight_stride, const int32_t* t_idx,
+                                        const int32_t* release_idx, float dt_seconds,
+                                        const glide_footprint_grid* grid, float* footprint, void* stream);
+
+/* --- Emanuel convection ------------------------------------------------------------
+ * EmanuelReducedConvection.maybe_convect (src/lpdm/convection/emanuel.py:570-716)
+ * and _redistribute_particles (:720-805): bbox-mean column, FP64 column build
+ * (LCL/LNB/CAPE, non-divergent mass-flux matrix, backward transition CDF), then
+ * per-particle transposed-column sampling. */
+glide_status glide_convect_scratch_bytes(int32_t nz, size_t* bytes);
+glide_status glide_convect(const glide_convect_args* args, void* stream);
+
+/* Reads the column result left in the scratch buffer by the last glide_convect
+ * on it (synchronises the stream): fires, i_lcl, i_lnb, cape, dtv, m_b. */
+glide_status glide_convect_column_info(const void* scratch, int32_t nz, void* stream, int32_t* fires,
+                                       int32_t* i_lcl, int32_t* i_lnb, double* cape, double* dtv, double* m_b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLIDE_B200_H */

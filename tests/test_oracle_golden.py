@@ -1,0 +1,145 @@
+"""The oracle against the reference's own outputs (golden fixtures made by
+``tests/golden/make_golden.py`` from the reference implementation).
+
+The first step must agree to the last bit or two; afterwards the trajectories
+of a few particles drift apart through ulp-level differences of the
+transcendental functions (numpy vs torch's SIMD kernels), which the
+turbulence dynamics amplify (regime switches on h/L = +-1, the BL-top
+free-troposphere switch, the integer substep count). Counts, the alive mask
+and the footprint are compared exactly or by ensemble tolerances.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from fixtures import load_run, oracle_kwargs
+from oracle import convection as oconv
+from oracle import hanna as oh
+from oracle.runtime import run_batch
+
+GOLDEN_UNITS = None
+
+
+def units():
+    global GOLDEN_UNITS
+    if GOLDEN_UNITS is None:
+        from fixtures import GOLDEN
+
+        GOLDEN_UNITS = dict(np.load(GOLDEN / "units.npz"))
+    return GOLDEN_UNITS
+
+
+def rel_err(a, b, floor=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+F = np.float32
+
+
+def test_in_bl_sigma_TL_matches_reference():
+    u = units()
+    out = oh.in_bl_sigma_TL(u["z"], u["blh"], u["ustar"], u["w_star"], u["hol"], u["lat"], F)
+    for k in range(6):
+        assert rel_err(out[k], u["in_bl"][k]).max() < 2e-6, k
+
+
+def test_stability_functions_match_reference():
+    u = units()
+    L = oh.obukhov_length(u["ustar"], u["shf"], u["tsfc"], u["sp"], F)
+    ref = u["obukhov"]
+    assert np.array_equal(np.isinf(L), np.isinf(ref))
+    fin = np.isfinite(ref)
+    assert rel_err(L[fin], ref[fin]).max() < 2e-6
+    assert rel_err(oh.convective_velocity(u["blh"], u["shf"], u["tsfc"], u["sp"], F), u["wstar"]).max() < 2e-6
+    assert rel_err(oh.coriolis_parameter(u["lat"], F), u["coriolis"], 1e-9).max() < 2e-6
+    assert rel_err(oh.surface_layer_sigma_w(u["z"], u["ustar"], L, F), u["sl_sigma_w"]).max() < 2e-6
+
+
+def test_free_troposphere_closure_matches_reference():
+    u = units()
+    kz = oh.free_trop_diffusivity(np.maximum(u["z"], F(1.0)), u["shear"], u["ri"], F)
+    assert rel_err(kz, u["kz"]).max() < 2e-6
+    sw, tl = oh.free_trop_sigma_TL(kz, u["n2"], F)
+    assert rel_err(sw, u["ft_sw"]).max() < 2e-6
+    assert rel_err(tl, u["ft_tl"]).max() < 2e-6
+
+
+def _unit_window():
+    u = units()
+    w = {n: u[f"u_met_{n}"][0:2] for n in ("u", "v", "w", "t", "q", "blh", "sp", "ustar", "shf")}
+    lev = u["u_met_levels"]
+    w["height"] = np.broadcast_to(lev.astype(F).reshape(-1, 1, 1), w["u"].shape[1:]).copy()
+    w.update(level=lev, p_hpa=u["u_met_p_hpa"], lon=u["u_met_lon"], lat=u["u_met_lat"])
+    return w
+
+
+def test_support_stacks_match_reference():
+    u = units()
+    w = _unit_window()
+    inp = oh.build_step_inputs(w, oh.HannaParams(meander_enabled=True), F)
+    assert rel_err(inp.ft_fields, u["stack_ft"]).max() < 1e-5
+    assert rel_err(inp.density_fields[0], u["stack_density"][0]).max() < 1e-6
+    assert np.abs(inp.density_fields[1] - u["stack_density"][1]).max() < 1e-9
+    assert np.abs(inp.meander_fields - u["stack_meander"]).max() < 1e-5
+
+
+def test_grid_samplers_bit_match_reference():
+    u = units()
+    w = _unit_window()
+    inp = oh.build_step_inputs(w, oh.HannaParams(meander_enabled=True), F)
+    gb = inp.gb
+    xn, yn, zn = oh.normalize_coords(u["s_lon"], u["s_lat"], u["s_z"], gb, F)
+    tri = oh.trilinear(u["stack_ft"], xn, yn, zn, F)
+    assert np.array_equal(tri, u["sample_tri"])
+    bil = oh.bilinear_at(w["blh"][0], gb.lon_first, gb.lon_last, gb.lat_first, gb.lat_last, u["s_lon"], u["s_lat"], F)
+    assert np.array_equal(bil, u["sample_bil"])
+    assert np.array_equal(oh.lerp(w["blh"][0], w["blh"][1], 0.3333, F), u["lerp_blh"])
+
+
+def test_emanuel_column_matches_reference():
+    u = units()
+    i_lcl, i_lnb, cape, dtv = oconv.compute_lcl_lnb_cape(u["c_t"], u["c_q"], u["c_p"], F)
+    ref = u["c_out"]
+    assert (i_lcl, i_lnb) == (int(ref[0]), int(ref[1]))
+    assert abs(cape - ref[2]) / ref[2] < 1e-4
+    assert abs(dtv - ref[3]) < 1e-4
+    fm = oconv.compute_mass_flux_matrix(u["c_p"], i_lcl, i_lnb, 0.05 * 3600.0, F)
+    assert np.abs(fm - u["c_fmass"]).max() <= 1e-6 * np.abs(u["c_fmass"]).max()
+    assert rel_err(oconv.layer_masses(u["c_p"], F), u["c_layer_mass"]).max() < 1e-6
+    # non-divergence (emanuel.py:429-470): row sums == column sums
+    assert np.allclose(fm.sum(axis=1), fm.sum(axis=0), rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.parametrize("name", ["run_small", "run_c0"])
+def test_first_step_matches_reference(name):
+    run = load_run(name)
+    res = run_batch(**oracle_kwargs(run), max_steps=1)
+    assert int(run["snap_steps"][0]) == 0
+    ref = run["snap_particles"][0]
+    assert rel_err(res.particles[:3], ref[:3], 1e-3).max() < 2e-6
+
+
+@pytest.mark.parametrize("name", ["run_small", "run_c0"])
+def test_batch_matches_reference(name):
+    run = load_run(name)
+    res = run_batch(**oracle_kwargs(run))
+    assert res.n_steps == int(run["n_steps"])
+    assert np.array_equal(res.active_per_step, run["out_active"])
+    assert np.array_equal(res.escaped_per_step, run["out_escaped"])
+    assert np.array_equal(res.alive, run["out_alive"])
+    if len(run["out_conv"]):
+        assert [m for _, f, m in res.convection] == [int(m) for _, m in run["out_conv"][1:]] or \
+            [m for _, f, m in res.convection] == [int(m) for _, m in run["out_conv"]]
+    ref = run["out_particles"]
+    scale = np.maximum(np.abs(ref[:3]), np.array([[1.0], [1.0], [10.0]]))
+    err = (np.abs(res.particles[:3] - ref[:3]) / scale).max(axis=0)
+    # most trajectories stay within 1e-5 relative of the reference
+    assert np.mean(err < 1e-5) > 0.5, np.mean(err < 1e-5)
+    assert np.median(err) < 1e-5
+    fp, rfp = res.footprint, run["out_footprint"]
+    assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 5e-3
+    assert abs(fp.sum() - rfp.sum()) / rfp.sum() < 1e-3
