@@ -1,0 +1,483 @@
+"""Benchmark of the B200 particle-step engine on the single-site EUROPE-box workload.
+
+Workload (one B200): one release at 100 m AGL of 200,000 particles over a 1 h
+release window, integrated 24 h backward at dt = 30 s (2,880 outer steps) with
+the Hanna scheme (max_substeps 6), meander on, Emanuel convection once per
+met window, a 24 x 281 x 401 time_ago x lat x lon footprint (0-100 m layer),
+on seeded synthetic met of 60 x 281 x 401 cells (0.25 deg, 26 hourly
+snapshots, float32). A bench step is one met window: 120 outer steps of the
+whole particle set, including the window's met packing and convection.
+
+``value``: particle-steps/s (particles x outer steps / device time), met
+resident in HBM. ``e2e``: the same job through the public runtime with the met
+snapshots in pinned host memory: every step copies its new snapshot to the
+device and reads back the window's diagnostics and footprint slice.
+
+``--impl reference``: the reference algorithm's CPU implementation (the numpy
+oracle port, all host cores, particle-parallel) on the same workload, timed on
+a bounded sample per step.
+
+Multi-GPU (torchrun): every rank runs its own release (replicas, weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from datetime import UTC, datetime, timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_PARTICLES = 200_000
+DT_S = 30.0
+SIM_LENGTH_S = 24 * 3600.0
+RELEASE_HEIGHT_M = 100.0
+SITE = (-5.0, 52.0)
+# algorithmic bytes per particle-step (met gathers 200 values x b + 86 B of state, footprint, flags)
+B_ALG = {"f32": 200 * 4 + 86, "bf16": 200 * 2 + 86, "f16": 200 * 2 + 86}
+METRIC = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--met", default="f32", choices=["f32", "bf16", "f16"])
+    ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n_particles: int, rank: int = 0):
+    from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.synthetic import config_met_spec
+
+    spec = config_met_spec(1, n_snapshots=26)
+    t0 = spec.start_time
+    release_time = t0 + timedelta(hours=23)
+    rel_end = release_time + timedelta(hours=1)
+    rng = np.random.default_rng(20261204 + rank)
+    lon, lat = SITE[0] + 2.0 * rank, SITE[1] - 1.0 * rank
+    particles = np.stack([np.full(n_particles, lon), np.full(n_particles, lat), np.full(n_particles, RELEASE_HEIGHT_M),
+                          np.full(n_particles, 1.0 / n_particles)], axis=1).astype(np.float32)
+    rel_off = rng.uniform(0.0, 3600.0, n_particles).astype(np.float32)
+    win_end = np.full(n_particles, 3600.0, dtype=np.float32)
+    ridx = np.zeros(n_particles, dtype=np.int32)
+    cfg = dict(
+        spec=spec, particles=particles, rel_off=rel_off, win_end=win_end, ridx=ridx,
+        batch_start=release_time, cursor_start=rel_end, terminus=rel_end - timedelta(seconds=SIM_LENGTH_S),
+        hanna=HannaConfig(meander_enabled=True, max_substeps=6),
+        emanuel=EmanuelConfig(),
+        footprint=FootprintSpec((-60.125, 40.125), (9.875, 80.125), 401, 281, (0.0, 100.0), 24, 1),
+        domain=DomainSpec((-60.0, 40.0), (10.0, 80.0), 20000.0),
+    )
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+            self.f.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the oracle port, particle-parallel over processes
+# ---------------------------------------------------------------------------
+
+
+def prepare_cpu_sample(syn, cfg, n_particles: int) -> str:
+    """Saves the met window and particles the CPU sample needs (window [23 h, 24 h]) to an
+    .npz in shared memory for the worker processes. The sample is the second and
+    third outer steps of that window: per-window work (support stacks, convection)
+    is excluded from the CPU timing."""
+    import tempfile
+
+    h = syn.window_index(cfg["cursor_start"] - timedelta(seconds=DT_S))
+    f0, f1 = syn.fields[h], syn.fields[h + 1]
+    arrs = {f"w_{k}": np.stack([f0[k].cpu().numpy(), f1[k].cpu().numpy()]) for k in f0}
+    arrs.update(height=syn.height_agl.cpu().numpy(), level=syn.levels, p_hpa=syn.pressure_level_hpa, lon=syn.lon,
+                lat=syn.lat, t_start=np.array(syn.times[h].timestamp()), t_end=np.array(syn.times[h + 1].timestamp()),
+                particles=cfg["particles"][:n_particles], rel_off=cfg["rel_off"][:n_particles],
+                win_end=cfg["win_end"][:n_particles],
+                batch_start=np.array(cfg["batch_start"].timestamp()),
+                cursor=np.array((cfg["cursor_start"] - timedelta(seconds=2 * DT_S)).timestamp()),
+                terminus=np.array(cfg["terminus"].timestamp()))
+    d = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    fd, path = tempfile.mkstemp(suffix=".npz", prefix="glide_cpu_", dir=d)
+    os.close(fd)
+    np.savez(path, **arrs)
+    return path
+
+
+_CPU_CACHE: dict = {}
+
+
+def _cpu_chunk(args):
+    path, lo, hi, n_steps, seed = args
+    from oracle.convection import EmanuelParams
+    from oracle.hanna import HannaParams, StepNoise
+    from oracle.runtime import DomainSpec, GridSpec, run_batch
+
+    z = np.load(path)
+    ts = lambda v: datetime.fromtimestamp(float(v), tz=UTC)  # noqa: E731
+    w = {k[2:]: z[k] for k in z.files if k.startswith("w_")}
+    w.update(height=z["height"], level=z["level"], p_hpa=z["p_hpa"], lon=z["lon"], lat=z["lat"],
+             time_start=ts(z["t_start"]), time_end=ts(z["t_end"]))
+    n = hi - lo
+    rng = np.random.default_rng(seed)
+
+    def noise_fn(step):
+        return StepNoise(rng.standard_normal((6, 3, n), dtype=np.float32), rng.standard_normal((2, n), dtype=np.float32))
+
+    kw = {}
+    cache = _CPU_CACHE.setdefault(path, {})
+    if not cache:  # per-window support stacks, built once per process (not timed)
+        from oracle.hanna import build_step_inputs
+
+        cache.update(key=datetime.fromtimestamp(float(z["t_start"]), tz=UTC), win=w,
+                     inp=build_step_inputs(w, HannaParams(meander_enabled=True, max_substeps=6), np.float32))
+    t = time.perf_counter()
+    run_batch(get_window=lambda hk: w, particles=z["particles"][lo:hi].T.copy(), rel_off=z["rel_off"][lo:hi],
+              win_end_off=z["win_end"][lo:hi], release_idx=np.zeros(n, dtype=np.int64),
+              batch_start=ts(z["batch_start"]), cursor_start=ts(z["cursor"]), cursor_terminus=ts(z["terminus"]),
+              sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S, params=HannaParams(meander_enabled=True, max_substeps=6),
+              grid=GridSpec((-60.125, 40.125), (9.875, 80.125), 401, 281, (0.0, 100.0), 24, 1),
+              domain=DomainSpec((-60.0, 40.0), (10.0, 80.0), 20000.0), noise_fn=noise_fn,
+              emanuel=EmanuelParams(), conv_uniforms_fn=lambda s: (rng.random(n, dtype=np.float32),
+                                                                   rng.random(n, dtype=np.float32)),
+              max_steps=n_steps, inputs_cache=cache, convect_first=False, **kw)
+    return time.perf_counter() - t
+
+
+def cpu_oracle_rate(path: str, n_particles: int, n_steps: int, workers: int) -> tuple[float, float]:
+    """(particle-steps/s, seconds) of the oracle on ``workers`` spawned processes; the
+    sample includes the window's support-stack build and convection column."""
+    import multiprocessing as mp
+
+    edges = np.linspace(0, n_particles, workers + 1).astype(int)
+    tasks = [(path, int(edges[i]), int(edges[i + 1]), n_steps, 1000 + i) for i in range(workers)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        pool.map(_cpu_chunk, [(path, 0, 64, 1, 7)] * workers)  # import + first-touch warm-up
+        t = time.perf_counter()
+        pool.map(_cpu_chunk, tasks)
+        wall = time.perf_counter() - t
+    return n_particles * n_steps / wall, wall
+
+
+def _cpu_met(cfg):
+    import torch
+
+    from glide_b200.synthetic import SyntheticMet
+
+    return SyntheticMet(cfg["spec"], device="cuda" if torch.cuda.is_available() else "cpu")
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    n_sample_steps = 2
+    cfg = workload(args.particles)
+    path = prepare_cpu_sample(_cpu_met(cfg), cfg, args.particles)
+    try:
+        rates = []
+        for _ in range(min(args.warmup, 1)):
+            cpu_oracle_rate(path, args.particles, 1, workers)
+        for _ in range(args.steps):
+            rates.append(cpu_oracle_rate(path, args.particles, n_sample_steps, workers)[0])
+    finally:
+        os.unlink(path)
+    value = float(statistics.median(rates))
+    sample = f"{args.particles} particles x {n_sample_steps} outer steps per step, oracle port on {workers} processes"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.particles * n_sample_steps / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "single-site 24 h backward, 200k particles, 60x281x401 met, dt 30 s"},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+
+
+def main() -> None:
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from glide_b200.runtime import BatchRunner, ParticleState
+    from glide_b200.synthetic import SyntheticMet
+    from glide_b200.window import grid_from_synthetic, window_from_synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    cfg = workload(args.particles, rank)
+    syn = SyntheticMet(cfg["spec"], device=dev)
+    grid = grid_from_synthetic(syn).to_device(dev)
+    n_windows_total = 25
+    if args.warmup + args.steps > n_windows_total:
+        raise SystemExit(f"warmup + steps must be <= {n_windows_total} windows (the 24 h job)")
+
+    def make_runner(provider):
+        return BatchRunner(grid=grid, window_provider=provider, hanna=cfg["hanna"], footprint=cfg["footprint"],
+                           domain=cfg["domain"], emanuel=cfg["emanuel"], met_dtype=args.met, device=dev,
+                           seed=1234 + rank)
+
+    def fresh_state():
+        return ParticleState.from_particles(cfg["particles"], cfg["rel_off"], cfg["win_end"], cfg["ridx"], dev)
+
+    runner = make_runner(lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid))
+    kw = dict(batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"], cursor_terminus=cfg["terminus"],
+              sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    # instrument the step-kernel launches with events on the launching stream
+    import glide_b200._abi as abi
+
+    stream = torch.cuda.current_stream()
+    kernel_events: list = []
+    real_step = abi.lib.glide_step
+
+    def timed_step(a, s):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = real_step(a, s)
+        e1.record(stream)
+        if record_kernels:
+            kernel_events.append((e0, e1))
+        return rc
+
+    abi.lib.glide_step = timed_step
+    record_kernels = False
+    run = runner.start(fresh_state(), **kw)
+    for _ in range(args.warmup):
+        run.step_window()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    steps_per_window = []
+    win_events = []
+    with ClockSampler(local) as clocks:
+        record_kernels = True
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            j0, j1 = run.windows[run.next_window]
+            e0.record(stream)
+            run.step_window()
+            e1.record(stream)
+            win_events.append((e0, e1))
+            steps_per_window.append(j1 - j0)
+        torch.cuda.synchronize()
+        record_kernels = False
+    if world > 1:
+        dist.barrier()
+    t_dev = sum(a.elapsed_time(b) for a, b in win_events) / 1e3
+    t_kernel = sum(a.elapsed_time(b) for a, b in kernel_events) / 1e3
+    n_kernel_launches = len(kernel_events)
+    out = run.finish() if run.done else None
+    status = int(run.status.item())
+    t_max = t_dev
+    if world > 1:
+        tt = torch.tensor([t_dev], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    n_outer = sum(steps_per_window)
+    p_steps = args.particles * n_outer
+    value = world * p_steps / t_max
+    ms_per_step = 1e3 * t_max / args.steps
+
+    # ---- end to end: met in pinned host memory, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, world)
+
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        achieved = B_ALG[args.met] * p_steps / t_kernel / 1e9
+        clk = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.met, "data": "synthetic",
+            "config": {"workload": "single-site 24 h backward, 200k particles, 60x281x401 met, dt 30 s",
+                       "particles": args.particles, "outer_steps_per_step": n_outer / args.steps,
+                       "met_storage": args.met, "meander": True, "convection": "emanuel_reduced",
+                       "max_substeps": 6, "step": "one met window (pack + convection + fused steps)",
+                       "l2": "flushed (256 MB write) before every timed step; met bricks 440 MB > L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "step_kernel", "bytes_per_particle_step": B_ALG[args.met],
+                         "kernel_time_share": t_kernel / t_dev},
+            "clocks": clk,
+            "gpu_launches": n_kernel_launches + 6 * args.steps,
+            "status": status,
+        }
+        if e2e is not None:
+            line["e2e"] = e2e
+        if not args.no_cpu_baseline and world == 1:
+            workers = os.cpu_count() or 1
+            path = prepare_cpu_sample(syn, cfg, args.particles)
+            try:
+                rate, wall = cpu_oracle_rate(path, args.particles, 2, workers)
+            finally:
+                os.unlink(path)
+            line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": workers, "kind": "port",
+                                    "sample": f"{args.particles} particles x 2 outer steps (oracle port, "
+                                              f"{workers} processes, {wall:.1f} s)"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, world) -> dict:
+    import torch
+
+    from glide_b200.window import Snapshot, WindowFields
+
+    lowest = int(np.argmin(syn.levels))
+    names3, names2 = ("u", "v", "w", "t", "q"), ("blh", "sp", "ustar", "shf")
+    host = []
+    for f in syn.fields:
+        host.append({k: f[k].to("cpu").pin_memory() for k in names3 + names2})
+    slots: dict = {}
+
+    def to_device(h):
+        if h in slots:
+            return slots[h]
+        if len(slots) >= 2:  # the cursor walks backward: drop the latest snapshot
+            slots.pop(max(slots))
+        d = {k: v.to(dev, non_blocking=True) for k, v in host[h].items()}
+        d["t_lowest"] = d["t"][lowest]
+        slots[h] = Snapshot(syn.times[h], d)
+        return slots[h]
+
+    copied = []
+
+    def provider(hk):
+        h = syn.window_index(hk)
+        before = set(slots)
+        ws, we = to_device(h), to_device(h + 1)
+        copied.append(len(set(slots) - before))
+        return WindowFields(ws, we, grid, None)
+
+    runner = make_runner(provider)
+    run = runner.start(fresh_state(), **kw)
+    for _ in range(args.warmup):
+        run.step_window()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    snap_bytes = sum(v.numel() * 4 for v in host[0].values())
+    h2d = 0
+    d2h = 0
+    copied.clear()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    n_outer = 0
+    for _ in range(args.steps):
+        j0, j1 = run.windows[run.next_window]
+        run.step_window()
+        esc = run.esc[j0:j1].to("cpu")
+        act = run.act[j0:j1].to("cpu")
+        tbin = min(int((3600.0 - run.steps[j1 - 1].cursor_off) // 3600.0), run.footprint.shape[1] - 1)
+        fp_slice = run.footprint[:, max(tbin, 0)].to("cpu")
+        d2h += esc.numel() * 4 + act.numel() * 4 + fp_slice.numel() * 4
+        n_outer += j1 - j0
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt.item())
+    h2d = sum(copied) * snap_bytes
+    return {"value": world * args.particles * n_outer / t, "unit": METRIC,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+
+
+if __name__ == "__main__":
+    main()

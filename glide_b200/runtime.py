@@ -262,6 +262,14 @@ class BatchRun:
             raise ValueError(f"window provider returned {wf.time_start} for hour {first.hour}")
         packed = r.packed_for(wf, stream)
         noise = r.noise_provider(list(range(j0, j1))) if r.noise_provider is not None else None
+        if noise is not None:  # the kernel indexes these buffers: check their extents first
+            sub, mea = noise
+            want = (j1 - j0, r.hanna.max_substeps, 3, self.state.n)
+            if tuple(sub.shape) != want or sub.dtype != torch.float32 or not sub.is_contiguous():
+                raise ValueError(f"injected substep noise must be contiguous float32 {want}, got {tuple(sub.shape)}")
+            if r.hanna.meander_enabled and (mea is None or tuple(mea.shape) != (j1 - j0, 2, self.state.n)
+                                            or mea.dtype != torch.float32 or not mea.is_contiguous()):
+                raise ValueError("injected meander noise must be contiguous float32 (steps, 2, n)")
         sh = stream_handle(stream)
         n = j1 - j0
         if r.emanuel is not None:
@@ -301,6 +309,8 @@ class BatchRun:
         a.closure_c, a.trigger_dtv_k = e.closure_c, e.trigger_dtv_k
         a.min_cape_j_kg, a.min_cloud_depth_m = e.min_cape_j_kg, e.min_cloud_depth_m
         u = r.conv_uniform_provider(j) if r.conv_uniform_provider is not None else None
+        if u is not None and (tuple(u.shape) != (2, s.n) or u.dtype != torch.float32 or not u.is_contiguous()):
+            raise ValueError(f"injected convection uniforms must be contiguous float32 (2, {s.n})")
         a.uniforms = None if u is None else u.data_ptr()
         a.seed = r.seed
         a.scratch = self.conv_scratch.data_ptr()

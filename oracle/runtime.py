@@ -145,12 +145,15 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
               noise_fn: Callable[[int], StepNoise], emanuel: conv.EmanuelParams | None = None,
               conv_uniforms_fn: Callable[[int], tuple[np.ndarray, np.ndarray]] | None = None,
               dtype=np.float32, conv_dtype=None, max_steps: int | None = None,
-              init_state: dict | None = None, init_alive=None, step_offset: int = 0) -> BatchResult:
+              init_state: dict | None = None, init_alive=None, step_offset: int = 0,
+              inputs_cache: dict | None = None, convect_first: bool = True) -> BatchResult:
     """The static cursor loop of ``main._run`` for one batch (main.py:1382-1477).
 
     ``init_state`` / ``init_alive`` / ``step_offset`` resume a batch mid-way: the
     loop starts at ``cursor_start`` from that state and numbers its steps from
-    ``step_offset`` (the noise rows)."""
+    ``step_offset`` (the noise rows). ``inputs_cache`` keeps the per-window support
+    stacks across calls; ``convect_first=False`` treats the first window as already
+    convected (a resumed mid-window start)."""
     dt = dtype
     conv_dt = conv_dtype or dtype
     n = particles.shape[1]
@@ -167,8 +170,8 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
     win_end_off = win_end_off.astype(dt)
     res = BatchResult(p, state, alive, fp.reshape(grid.shape))
     bstart = batch_start.timestamp()
-    cache: dict = {}
-    last_bracket = None
+    cache: dict = inputs_cache if inputs_cache is not None else {}
+    last_bracket = None if convect_first else hour_floor(cursor_start)
     t_cursor = cursor_start
     step = 0
     while t_cursor > cursor_terminus:

@@ -1,0 +1,67 @@
+"""The C-ABI library loads without a GPU, exports every symbol ``include/glide_b200.h``
+declares, agrees with the ctypes struct layouts, and rejects invalid arguments
+with a status and an error text before touching the device."""
+
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from glide_b200 import _abi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "glide_b200.h"
+
+
+def declared_functions() -> set[str]:
+    text = HEADER.read_text()
+    return set(re.findall(r"^\s*(?:glide_status|int32_t)\s+(glide_\w+)\s*\(", text, re.M))
+
+
+def test_header_declares_what_the_binding_binds():
+    assert declared_functions() == set(_abi.SIGNATURES)
+
+
+def test_every_symbol_is_exported():
+    lib = C.CDLL(str(_abi.LIB_PATH))
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_struct_layouts_match():
+    sizes = (C.c_size_t * 6)()
+    assert _abi.lib.glide_abi_struct_sizes(sizes, 6) == 0
+    assert list(sizes) == [C.sizeof(s) for s in _abi.STRUCTS]
+    assert _abi.lib.glide_version() >= 100
+
+
+def test_invalid_arguments_are_rejected_without_a_device():
+    assert _abi.lib.glide_step(None, None) == 1
+    assert "NULL" in _abi.last_error()
+    a = _abi.StepArgs()
+    a.n = 10
+    a.n_steps = 1
+    assert _abi.lib.glide_step(C.byref(a), None) == 1
+    assert "NULL" in _abi.last_error()
+    a.n_steps = 0
+    assert _abi.lib.glide_step(C.byref(a), None) == 1
+    assert "n_steps" in _abi.last_error()
+    w = _abi.WindowDesc()
+    assert _abi.lib.glide_window_pack(C.byref(w), None) == 1
+    c = _abi.ConvectArgs()
+    assert _abi.lib.glide_convect(C.byref(c), None) == 1
+    nb = C.c_size_t()
+    assert _abi.lib.glide_convect_scratch_bytes(1, C.byref(nb)) == 1
+    assert _abi.lib.glide_convect_scratch_bytes(60, C.byref(nb)) == 0
+    assert nb.value == 8 * (8 + 4 * 60 + 60 * 60)
+    wb, sb, pb = C.c_size_t(), C.c_size_t(), C.c_size_t()
+    assert _abi.lib.glide_window_packed_bytes(60, 281, 401, 0, C.byref(wb), C.byref(sb), C.byref(pb)) == 0
+    assert wb.value == 60 * 281 * 401 * 32 and sb.value == 281 * 401 * 64
+    assert _abi.lib.glide_window_packed_bytes(60, 281, 401, 7, C.byref(wb), C.byref(sb), C.byref(pb)) == 3
+
+
+def test_check_raises_with_text():
+    with pytest.raises(_abi.GlideError, match="args is NULL"):
+        _abi.check(_abi.lib.glide_step(None, None), "glide_step")
