@@ -58,15 +58,21 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--snapshots", type=int, default=26,
+                    help="generate only the last N hourly snapshots (small profiling cases)")
     return ap.parse_args()
 
 
-def workload(n_particles: int, rank: int = 0):
+def workload(n_particles: int, rank: int = 0, n_snapshots: int = 26):
+    import dataclasses
+
     from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
     from glide_b200.synthetic import config_met_spec
 
     spec = config_met_spec(1, n_snapshots=26)
     t0 = spec.start_time
+    if n_snapshots < 26:  # same hours at the end of the job, fewer generated before them
+        spec = dataclasses.replace(spec, n_snapshots=n_snapshots, start_time=t0 + timedelta(hours=26 - n_snapshots))
     release_time = t0 + timedelta(hours=23)
     rel_end = release_time + timedelta(hours=1)
     rng = np.random.default_rng(20261204 + rank)
@@ -289,10 +295,10 @@ def main() -> None:
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-    cfg = workload(args.particles, rank)
+    cfg = workload(args.particles, rank, args.snapshots)
     syn = SyntheticMet(cfg["spec"], device=dev)
     grid = grid_from_synthetic(syn).to_device(dev)
-    n_windows_total = 25
+    n_windows_total = args.snapshots - 1
     if args.warmup + args.steps > n_windows_total:
         raise SystemExit(f"warmup + steps must be <= {n_windows_total} windows (the 24 h job)")
 
