@@ -15,6 +15,8 @@
 //
 // Scratch layout (doubles): header[8] | t[nz] | q[nz] | h[nz] | h_asc[nz] | cum[nz][nz]
 //   header: fires, i_lcl, i_lnb, cape, dtv, m_b, ascending, -
+#include <mutex>
+
 #include "common.cuh"
 #include "glide_internal.h"
 
@@ -377,4 +379,78 @@ extern "C" glide_status glide_convect_column_info(const void* scratch, int32_t n
     if (dtv) *dtv = h[4];
     if (m_b) *m_b = h[5];
     return GLIDE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant: the scratch is a file-scope device array instead of
+// a caller buffer. Host code cannot use the array's name as a device address;
+// each device's address is looked up once (cudaGetSymbolAddress, with that
+// device current) and passed to the kernels.
+// ---------------------------------------------------------------------------
+
+namespace glide {
+
+constexpr int NOALLOC_MAX_NZ = GLIDE_CONVECT_NOALLOC_MAX_NZ;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_convect_scratch[8 + 4 * NOALLOC_MAX_NZ + NOALLOC_MAX_NZ * NOALLOC_MAX_NZ];
+
+static std::mutex g_scratch_mu;
+static double* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+
+static glide_status noalloc_scratch(double** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "glide_convect_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return set_error(GLIDE_ERR_UNSUPPORTED, "glide_convect_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_convect_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "glide_convect_noalloc: cudaGetSymbolAddress");
+        g_scratch_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return GLIDE_OK;
+}
+
+}  // namespace glide
+
+extern "C" glide_status glide_convect_noalloc(const glide_convect_args* a, void* stream) {
+    if (!a) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: args is NULL");
+    if (a->nz > NOALLOC_MAX_NZ)
+        return set_error(GLIDE_ERR_INVALID_ARG,
+                         "glide_convect_noalloc: nz = %d exceeds the %d levels of its static scratch "
+                         "(use glide_convect with a caller scratch buffer)", a->nz, NOALLOC_MAX_NZ);
+    if (a->nz < 2 || a->ny < 1 || a->nx < 1)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: grid out of range (2 <= nz)");
+    if (a->n < 0) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: n < 0");
+    if (!a->t[0] || !a->t[1] || !a->q[0] || !a->q[1] || !a->pressure_hpa || (!a->height3d && !a->height_level))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: NULL input");
+    if (a->n > 0 && (!a->z || (!a->active_mask && !a->rel_off)))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: NULL particle input");
+    if (a->z_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: z_stride < 1");
+    double* scratch = nullptr;
+    const glide_status st = noalloc_scratch(&scratch);
+    if (st != GLIDE_OK) return st;
+    ConvDev d;
+    d.n = a->n; d.z = a->z; d.zs = a->z_stride;
+    d.rel_off = a->rel_off; d.alive = a->alive; d.active_mask = a->active_mask;
+    d.sim_length = a->sim_length_s; d.sched = a->sched;
+    d.nz = a->nz; d.ny = a->ny; d.nx = a->nx;
+    d.t[0] = a->t[0]; d.t[1] = a->t[1]; d.q[0] = a->q[0]; d.q[1] = a->q[1];
+    d.h3 = a->height3d; d.hlev = a->height_level; d.p_hpa = a->pressure_hpa;
+    d.alpha = (double)a->alpha;
+    d.closure_c = a->closure_c; d.trigger_dtv = a->trigger_dtv_k; d.min_cape = a->min_cape_j_kg;
+    d.min_depth = a->min_cloud_depth_m;
+    d.uniforms = a->uniforms; d.seed_lo = (uint32_t)a->seed; d.seed_hi = (uint32_t)(a->seed >> 32);
+    d.scratch = scratch;
+    d.n_moved = a->n_moved;
+    cudaStream_t s = (cudaStream_t)stream;
+    column_reduce_kernel<<<a->nz, 512, 0, s>>>(d);
+    const int threads = a->nz <= 64 ? 64 : 128;
+    column_build_kernel<<<1, threads, sizeof(double) * 10 * (size_t)a->nz, s>>>(d);
+    if (a->n > 0) redistribute_kernel<<<(unsigned)((a->n + 255) / 256), 256, 0, s>>>(d);
+    return check_launch("glide_convect_noalloc");
 }

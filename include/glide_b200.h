@@ -196,6 +196,27 @@ glide_status glide_footprint_accumulate(int64_t n, const float* lon, const float
 glide_status glide_convect_scratch_bytes(int32_t nz, size_t* bytes);
 glide_status glide_convect(const glide_convect_args* args, void* stream);
 
+/* Maximum number of met levels that glide_convect_noalloc accepts. */
+#define GLIDE_CONVECT_NOALLOC_MAX_NZ 128
+
+/* glide_convect for callers that cannot allocate device memory. No counterpart
+ * in the reference: it exists for callers that must not call cudaMalloc, such as
+ * a serving loop that has already committed its whole HBM budget to particle
+ * state and footprints, a process whose framework allocator holds nearly all
+ * device memory (a raw cudaMalloc there fails or fragments the pool), or a
+ * foreign-language caller with no access to any device allocator. The caller
+ * still passes every input and output; args->scratch is ignored. The scratch
+ * lives in one static device array of the library, sized for at most
+ * GLIDE_CONVECT_NOALLOC_MAX_NZ levels (135 KB, held by every GPU that loads the
+ * library until exit); larger grids are rejected with GLIDE_ERR_INVALID_ARG.
+ * The first call on each device looks up that array's device address with the
+ * device current; make that first call before any stream capture. All calls
+ * share the array: two calls that may run at the same time on the GPU (streams
+ * not ordered with each other) race on it. Each call writes every part of the
+ * array it reads before reading it, so nothing needs clearing between calls.
+ * Allocates nothing. */
+glide_status glide_convect_noalloc(const glide_convect_args* args, void* stream);
+
 /* Reads the column result left in the scratch buffer by the last glide_convect
  * on it (synchronises the stream): fires, i_lcl, i_lnb, cape, dtv, m_b. */
 glide_status glide_convect_column_info(const void* scratch, int32_t nz, void* stream, int32_t* fires,
