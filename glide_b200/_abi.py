@@ -8,9 +8,11 @@ or stale library raises ``ImportError`` with the reason.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libglide_b200.so"
+# GLIDE_B200_LIBRARY may name another build of the same library (e.g. a debug build)
+LIB_PATH = Path(os.environ.get("GLIDE_B200_LIBRARY") or Path(__file__).resolve().parent / "libglide_b200.so")
 
 GLIDE_OK = 0
 GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
@@ -22,7 +24,8 @@ vp = C.c_void_p
 class Grid(C.Structure):
     _fields_ = [("nz", C.c_int32), ("ny", C.c_int32), ("nx", C.c_int32), ("ascending", C.c_int32),
                 ("lon_first", C.c_double), ("lon_last", C.c_double), ("lat_first", C.c_double),
-                ("lat_last", C.c_double), ("level_sorted", vp)]
+                ("lat_last", C.c_double), ("level_sorted", vp), ("level_lut", vp), ("lut_n", C.c_int32),
+                ("lut_inv_dz", C.c_float)]
 
 
 class WindowDesc(C.Structure):

@@ -46,30 +46,38 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
-    """Compile the library in place (next to this file) if a source is newer than it."""
-    if not force and not ptxas_info and not _stale():
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, out: Path | None = None,
+          extra_flags: list[str] | None = None) -> Path:
+    """Compile the library in place (next to this file) if a source is newer than it.
+    ``out`` / ``extra_flags`` build a variant elsewhere (always rebuilt)."""
+    lib_path = Path(out) if out is not None else LIB_PATH
+    if out is None and not force and not ptxas_info and not extra_flags and not _stale():
         return LIB_PATH
     nvcc = nvcc_path()
-    out_dir = PKG / "_build"
+    out_dir = (lib_path.parent / (lib_path.stem + "_build")) if out is not None else PKG / "_build"
     out_dir.mkdir(exist_ok=True)
     objs = []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     for src in SOURCES:
         obj = out_dir / (Path(src).stem + ".o")
-        cmd = [nvcc, *ARCH_FLAGS, *NVCC_FLAGS, *extra, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src),
+        flags = list(NVCC_FLAGS)
+        for f in extra_flags or []:
+            if f.startswith("-fmad="):
+                flags = [x for x in flags if not x.startswith("-fmad=")]
+            flags.append(f)
+        cmd = [nvcc, *ARCH_FLAGS, *flags, *extra, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src),
                "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
-    tmp = LIB_PATH.with_suffix(".so.tmp")
+    tmp = lib_path.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-cudart", "static", "-o", str(tmp), *objs]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":

@@ -105,11 +105,12 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
 // uniform in (0, 1): 24 random bits, centred in their bin
 __device__ __forceinline__ float u01(uint32_t x) { return ((x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 
-// two standard normals by the Box-Muller transform
+// two standard normals by the Box-Muller transform (hardware approximations of
+// log and sin/cos: relative errors ~1e-6, far below what a Gaussian sample needs)
 __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
-    const float r = sqrtf(-2.0f * logf(u01(a)));
+    const float r = __fsqrt_rn(-2.0f * __logf(u01(a)));
     float s, c;
-    sincospif(2.0f * u01(b), &s, &c);
+    __sincosf(6.2831853071795865f * u01(b) - 3.1415926535897932f, &s, &c);
     return make_float2(r * c, r * s);
 }
 
@@ -128,6 +129,9 @@ struct GridDev {
     float lat0, lat_span;
     float zmax_idx;        // float32(nz - 1)
     const float* level;    // ascending [nz]
+    const int32_t* lut;    // optional: lut[b] = searchsorted(level, b / lut_inv_dz)
+    int lut_n;
+    float lut_inv_dz;
 };
 
 __host__ inline GridDev make_grid_dev(const glide_grid& g) {
@@ -140,6 +144,9 @@ __host__ inline GridDev make_grid_dev(const glide_grid& g) {
     d.lat_span = (float)(g.lat_last - g.lat_first);
     d.zmax_idx = (float)(g.nz - 1);
     d.level = g.level_sorted;
+    d.lut = g.level_lut;
+    d.lut_n = g.lut_n;
+    d.lut_inv_dz = g.lut_inv_dz;
     return d;
 }
 
@@ -153,10 +160,22 @@ __device__ __forceinline__ float norm_h(float v, float v0, float span) {
 // normalised z through the piecewise-linear level lookup (gpu_engine.py:263-293)
 __device__ __forceinline__ float norm_z(float z, const GridDev& g) {
     const int n = g.nz;
-    int lo = 0, hi = n;
-    while (lo < hi) {  // searchsorted(level, z), left insertion
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(g.level + mid) < z) lo = mid + 1; else hi = mid;
+    int lo;
+    if (g.lut) {
+        // searchsorted is monotone in z, so the table entry of the bucket below z's
+        // (z * inv_dz may round up across a bucket edge) is a lower bound of the
+        // answer; scan forward to the leftmost level >= z (NaN: 0, as below)
+        const float fb = z * g.lut_inv_dz;
+        const int b = (fb >= 1.0f) ? min((int)fb, g.lut_n) - 1 : 0;
+        lo = __ldg(g.lut + b);
+        while (lo < n && __ldg(g.level + lo) < z) ++lo;
+    } else {
+        lo = 0;
+        int hi = n;
+        while (lo < hi) {  // searchsorted(level, z), left insertion
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(g.level + mid) < z) lo = mid + 1; else hi = mid;
+        }
     }
     const int iu = min(max(lo, 1), n - 1);
     const int il = iu - 1;

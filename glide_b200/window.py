@@ -43,6 +43,8 @@ class GridInfo:
     level_sorted_dev: torch.Tensor = field(repr=False, default=None)
     p_hpa_dev: torch.Tensor = field(repr=False, default=None)
     height_level_dev: torch.Tensor = field(repr=False, default=None)
+    level_lut_dev: torch.Tensor = field(repr=False, default=None)
+    lut_inv_dz: float = 0.0
 
     @property
     def shape(self) -> tuple[int, int, int]:
@@ -52,7 +54,22 @@ class GridInfo:
     def ascending(self) -> bool:
         return bool(self.level[-1] > self.level[0])
 
+    def level_lut(self, max_entries: int = 4096) -> tuple[np.ndarray, float]:
+        """Bucket table of the level search: ``lut[b] = searchsorted(level, b / inv_dz)``
+        (float32 levels, left insertion), buckets no wider than the thinnest layer."""
+        lv = np.sort(np.asarray(self.level, dtype=np.float32))
+        thinnest = float(np.min(np.diff(lv.astype(np.float64)))) if lv.size > 1 else 1.0
+        top = float(lv[-1]) if float(lv[-1]) > 0 else 1.0
+        n = int(min(max_entries, max(2, np.ceil(top / max(thinnest, 1e-3)) + 1)))
+        inv_dz = np.float32((n - 1) / top)
+        edges = (np.arange(n, dtype=np.float64) / np.float64(inv_dz)).astype(np.float32)
+        lut = np.searchsorted(lv, edges, side="left").astype(np.int32)
+        return lut, float(inv_dz)
+
     def to_device(self, device) -> GridInfo:
+        lut, inv = self.level_lut()
+        self.level_lut_dev = torch.as_tensor(lut, device=device)
+        self.lut_inv_dz = inv
         self.level_sorted_dev = torch.as_tensor(np.sort(np.asarray(self.level, dtype=np.float32)), device=device)
         self.p_hpa_dev = torch.as_tensor(np.asarray(self.pressure_level_hpa, dtype=np.float32), device=device)
         self.height_level_dev = torch.as_tensor(np.asarray(self.level, dtype=np.float32), device=device)
@@ -60,8 +77,11 @@ class GridInfo:
 
     def c_grid(self) -> _abi.Grid:
         nz, ny, nx = self.shape
+        lut = self.level_lut_dev
         return _abi.Grid(nz, ny, nx, 1 if self.ascending else 0, float(self.lon[0]), float(self.lon[-1]),
-                         float(self.lat[0]), float(self.lat[-1]), self.level_sorted_dev.data_ptr())
+                         float(self.lat[0]), float(self.lat[-1]), self.level_sorted_dev.data_ptr(),
+                         None if lut is None else lut.data_ptr(), 0 if lut is None else lut.numel(),
+                         self.lut_inv_dz)
 
 
 @dataclass

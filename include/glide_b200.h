@@ -43,6 +43,12 @@ typedef struct glide_grid {
     double lon_first, lon_last;  /* cell-centre coordinates of x = 0 and x = nx-1 */
     double lat_first, lat_last;  /* cell-centre coordinates of y = 0 and y = ny-1 */
     const float* level_sorted;   /* device [nz], AGL heights sorted ascending */
+    /* optional lookup table accelerating the level search: level_lut[b] =
+     * searchsorted(level_sorted, b / lut_inv_dz) for b in [0, lut_n); NULL = binary search.
+     * Results are identical either way. */
+    const int32_t* level_lut;
+    int32_t lut_n;
+    float lut_inv_dz;
 } glide_grid;
 
 /*
