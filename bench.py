@@ -419,47 +419,26 @@ def main() -> None:
 
 
 def run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, world) -> dict:
+    """The job through the public runtime with the met in pinned host memory: each
+    window's new snapshot is copied to the device by ``HostMetStreamer`` (prefetched
+    on a copy stream during the previous window); each step reads back the window's
+    diagnostics and the footprint slice of its time-ago bin."""
     import torch
 
-    from glide_b200.window import Snapshot, WindowFields
+    from glide_b200.window import HostMetStreamer
 
-    lowest = int(np.argmin(syn.levels))
-    names3, names2 = ("u", "v", "w", "t", "q"), ("blh", "sp", "ustar", "shf")
-    host = []
-    for f in syn.fields:
-        host.append({k: f[k].to("cpu").pin_memory() for k in names3 + names2})
-    slots: dict = {}
-
-    def to_device(h):
-        if h in slots:
-            return slots[h]
-        if len(slots) >= 2:  # the cursor walks backward: drop the latest snapshot
-            slots.pop(max(slots))
-        d = {k: v.to(dev, non_blocking=True) for k, v in host[h].items()}
-        d["t_lowest"] = d["t"][lowest]
-        slots[h] = Snapshot(syn.times[h], d)
-        return slots[h]
-
-    copied = []
-
-    def provider(hk):
-        h = syn.window_index(hk)
-        before = set(slots)
-        ws, we = to_device(h), to_device(h + 1)
-        copied.append(len(set(slots) - before))
-        return WindowFields(ws, we, grid, None)
-
-    runner = make_runner(provider)
+    names = HostMetStreamer.NAMES
+    host = [{k: f[k].to("cpu").pin_memory() for k in names} for f in syn.fields]
+    streamer = HostMetStreamer(lambda k: host[k], syn.times, grid, dev, lowest=int(np.argmin(syn.levels)))
+    runner = make_runner(streamer)
     run = runner.start(fresh_state(), **kw)
     for _ in range(args.warmup):
         run.step_window()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    snap_bytes = sum(v.numel() * 4 for v in host[0].values())
-    h2d = 0
+    b0 = streamer.bytes_copied
     d2h = 0
-    copied.clear()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -467,10 +446,10 @@ def run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, wor
     for _ in range(args.steps):
         j0, j1 = run.windows[run.next_window]
         run.step_window()
-        esc = run.esc[j0:j1].to("cpu")
-        act = run.act[j0:j1].to("cpu")
+        esc = run.esc[j0:j1].to("cpu", non_blocking=True)
+        act = run.act[j0:j1].to("cpu", non_blocking=True)
         tbin = min(int((3600.0 - run.steps[j1 - 1].cursor_off) // 3600.0), run.footprint.shape[1] - 1)
-        fp_slice = run.footprint[:, max(tbin, 0)].to("cpu")
+        fp_slice = run.footprint[:, max(tbin, 0)].to("cpu", non_blocking=True)
         d2h += esc.numel() * 4 + act.numel() * 4 + fp_slice.numel() * 4
         n_outer += j1 - j0
     e1.record(stream)
@@ -480,7 +459,7 @@ def run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, wor
         tt = torch.tensor([t], device=dev)
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t = float(tt.item())
-    h2d = sum(copied) * snap_bytes
+    h2d = streamer.bytes_copied - b0
     return {"value": world * args.particles * n_outer / t, "unit": METRIC,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
 

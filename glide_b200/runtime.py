@@ -281,6 +281,11 @@ class BatchRun:
         else:
             a = self._step_args(packed, j0, n, 0, 0, noise)
             _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+        prov = r.window_provider
+        if hasattr(prov, "window_done"):  # streaming provider: release this window, prefetch the next
+            prov.window_done(first.hour)
+            if not self.done:
+                prov.prefetch(self.steps[self.windows[self.next_window][0]].hour)
         return True
 
     def _convect(self, wf: WindowFields, j: int, stream) -> None:

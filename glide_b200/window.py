@@ -230,3 +230,103 @@ def window_from_arrays(fields: dict, h: int, times: list, grid: GridInfo, device
         f["t_lowest"] = f["t"][lowest]
         snaps.append(Snapshot(times[k], f))
     return WindowFields(snaps[0], snaps[1], grid, None)
+
+
+class HostMetStreamer:
+    """Streams hourly snapshots from (pinned) host memory to the device.
+
+    The device holds ``slots`` snapshot buffers. A window ``[h, h+1]`` needs two;
+    walking backward, the next window needs one new snapshot, which
+    ``prefetch(hour)`` copies on a side stream while the current window computes
+    (the device-side counterpart of the reference's ``MetPrefetcher``,
+    src/lpdm/main.py:791-889). A slot is overwritten only after the compute stream
+    has passed the point where its previous snapshot was last used.
+
+    ``host_snapshot(k)`` returns snapshot ``k`` as a dict of host tensors (3-D
+    ``[Z, Y, X]``: u, v, w, t, q; 2-D ``[Y, X]``: blh, sp, ustar, shf); ``times[k]``
+    is its time.
+    """
+
+    NAMES = ("u", "v", "w", "t", "q", "blh", "sp", "ustar", "shf")
+
+    def __init__(self, host_snapshot, times: list, grid: GridInfo, device, lowest: int = 0, slots: int = 3) -> None:
+        if slots < 3:
+            raise ValueError("need at least 3 snapshot slots (two in use, one being filled)")
+        self.host_snapshot = host_snapshot
+        self.times = list(times)
+        self.grid = grid
+        self.device = torch.device(device)
+        self.lowest = lowest
+        self.copy_stream = torch.cuda.Stream(device=self.device)
+        self.slots: list[dict] = []
+        self.slot_of: dict[int, int] = {}
+        self.ready: dict[int, torch.cuda.Event] = {}
+        self.free_after: list[torch.cuda.Event | None] = [None] * slots
+        self.n_slots = slots
+        self.bytes_copied = 0
+        self.t0 = self.times[0]
+
+    def _index(self, hour: datetime) -> int:
+        return int(round((hour - self.t0).total_seconds() / 3600.0))
+
+    def _alloc(self, like: dict) -> dict:
+        return {k: torch.empty(v.shape, dtype=torch.float32, device=self.device) for k, v in like.items()}
+
+    def _load(self, k: int, keep: set) -> None:
+        """Start copying snapshot k into a free slot (on the copy stream)."""
+        if k in self.slot_of or k < 0 or k >= len(self.times):
+            return
+        host = self.host_snapshot(k)
+        used = set(self.slot_of.values())
+        if len(self.slots) < self.n_slots:
+            self.slots.append(self._alloc(host))
+            slot = len(self.slots) - 1
+        else:
+            victims = [(s, kk) for kk, s in self.slot_of.items() if kk not in keep]
+            if not victims:
+                raise RuntimeError("no free snapshot slot")
+            slot, kk = max(victims, key=lambda v: v[1])  # the cursor walks backward: drop the latest
+            del self.slot_of[kk]
+            self.ready.pop(kk, None)
+        del used
+        ev_free = self.free_after[slot]
+        with torch.cuda.stream(self.copy_stream):
+            if ev_free is not None:
+                self.copy_stream.wait_event(ev_free)
+            for name, src in host.items():
+                self.slots[slot][name].copy_(src, non_blocking=True)
+                self.bytes_copied += src.numel() * src.element_size()
+            ev = torch.cuda.Event()
+            ev.record(self.copy_stream)
+        self.slot_of[k] = slot
+        self.ready[k] = ev
+
+    def _snapshot(self, k: int) -> Snapshot:
+        slot = self.slots[self.slot_of[k]]
+        torch.cuda.current_stream(self.device).wait_event(self.ready[k])
+        f = dict(slot)
+        f["t_lowest"] = f["t"][self.lowest]
+        return Snapshot(self.times[k], f)
+
+    def __call__(self, hour: datetime) -> WindowFields:
+        h = self._index(hour)
+        self._load(h + 1, {h, h + 1})
+        self._load(h, {h, h + 1})
+        return WindowFields(self._snapshot(h), self._snapshot(h + 1), self.grid, None)
+
+    def window_done(self, hour: datetime) -> None:
+        """Marks the point of the compute stream after which the window's snapshots
+        may be overwritten (called once the window's launches are issued)."""
+        h = self._index(hour)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        for k in (h, h + 1):
+            if k in self.slot_of:
+                self.free_after[self.slot_of[k]] = ev
+
+    def prefetch(self, hour: datetime) -> None:
+        """Starts the copy of the snapshots window ``hour`` needs, keeping the
+        current window's (the one after it in time) resident."""
+        h = self._index(hour)
+        self._load(h, {h, h + 1, h + 2})
+        self._load(h + 1, {h, h + 1, h + 2})
