@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
         vp = p.vp[i];
         wp = p.wp[i];
         if (p.meander) { um = p.um[i]; vm = p.vm[i]; }
-        rel = p.rel_off[i];
+        rel = p.rel_off ? p.rel_off[i] : 0.f;
         wend = p.win_end_off ? p.win_end_off[i] : 0.f;
         rid = p.release_idx ? p.release_idx[i] : 0;
         alive = p.alive ? (p.alive[i] != 0) : true;
@@ -558,8 +558,10 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (!a->sched && a->n_steps != 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: sched is NULL but n_steps = %d", a->n_steps);
     if (a->n == 0) return GLIDE_OK;
-    if (!a->lon || !a->lat || !a->z || !a->weight || !a->u_prime || !a->v_prime || !a->w_prime || !a->rel_off)
+    if (!a->lon || !a->lat || !a->z || !a->weight || !a->u_prime || !a->v_prime || !a->w_prime)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: a particle state pointer is NULL");
+    if (!a->active_mask && !a->rel_off)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: rel_off is NULL and no active_mask is given");
     if (a->meander_enabled && (!a->u_meander || !a->v_meander || !a->support_packed))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: meander enabled but meander state is NULL");
     if (!a->wind_packed || !a->surf_packed || !a->support_packed || !a->grid.level_sorted)

@@ -102,3 +102,101 @@ def oracle_from(run: GoldenRun, **kw):
 
 
 UTC_ = UTC
+
+
+def hourly_window(run: GoldenRun, h: int):
+    """The reference-format ``HourlyMetTensors`` of bracket ``[h, h+1]`` (host tensors,
+    2-D fields broadcast over Z)."""
+    from glide_b200.met import HourlyMetTensors, MetFieldMetadata
+
+    m = run.met
+    names = ("u", "v", "w", "blh", "sp", "t", "ustar", "shf", "q")
+    nz = m.fields["u"].shape[1]
+
+    def stack(k):
+        chans = []
+        for name in names:
+            f = torch.as_tensor(m.fields[name][k])
+            chans.append(f.unsqueeze(0).expand(nz, -1, -1) if f.dim() == 2 else f)
+        return torch.stack(chans)
+
+    md = MetFieldMetadata(lon=np.asarray(m.lon), lat=np.asarray(m.lat), level=np.asarray(m.levels),
+                          pressure_level_hpa=np.asarray(m.p_hpa), time_start=m.time(h), time_end=m.time(h + 1))
+    lev = torch.as_tensor(np.asarray(m.levels, dtype=np.float32)).view(-1, 1, 1)
+    return HourlyMetTensors(stack(h), stack(h + 1), md, names, lev.expand(nz, *m.fields["u"].shape[2:]))
+
+
+def run_plugin_loop(run: GoldenRun, device):
+    """The reference's static per-step runtime body (main.py:1382-1477) driving the
+    B200 plug-ins: HannaB200Scheme.step, EmanuelB200Convection.maybe_convect,
+    FootprintGridderB200.accumulate and the escape kill, with injected noise."""
+    from glide_b200.runtime import plan_steps
+    from glide_b200.schemes import FootprintGridderB200, get_convection_scheme, get_scheme
+
+    z = run.z
+    n = run.n
+    ms = int(z["max_substeps"])
+    seed, cseed = int(z["noise_seed"]), int(z["conv_seed"])
+
+    def noise(step):
+        from fixtures import step_noise
+
+        sub, mea = step_noise(seed, step, ms, n)
+        return torch.from_numpy(sub).to(device), torch.from_numpy(mea).to(device)
+
+    cur_step = {"k": 0}
+
+    def uniforms(_call):
+        u1, u2 = conv_uniforms(cseed, cur_step["k"], n)
+        return torch.from_numpy(np.stack([u1, u2])).to(device)
+
+    scheme = get_scheme("hanna_1982_b200", meander_enabled=bool(z["meander"]), max_substeps=ms,
+                        noise_provider=noise)
+    conv = (get_convection_scheme("emanuel_reduced_b200", uniform_provider=uniforms)
+            if bool(z["convection"]) else None)
+    nxy = z["grid_nxy"]
+    gridder = FootprintGridderB200(tuple(z["grid_lon"]), tuple(z["grid_lat"]), tuple(z["grid_z"]), int(nxy[2]),
+                                   int(nxy[1]), int(nxy[0]), n_releases=int(z["release_idx"].max()) + 1,
+                                   device=device)
+    particles = torch.as_tensor(z["particles0"].T.copy(), device=device)
+    state = scheme.initialize_state(n, device=device, dtype=torch.float32)
+    rel = torch.as_tensor(z["rel_off"], device=device)
+    wend = torch.as_tensor(z["win_end_off"], device=device)
+    ridx = torch.as_tensor(z["release_idx"], device=device)
+    alive = torch.ones(n, dtype=torch.bool, device=device)
+    L = float(z["sim_length_s"])
+    dl0, dl1 = (float(v) for v in z["dom_lon"])
+    da0, da1 = (float(v) for v in z["dom_lat"])
+    alt = float(z["dom_alt"])
+    esc, act = [], []
+    last_bracket = None
+    windows: dict = {}
+    steps = plan_steps(run.dt_("batch_start"), run.dt_("cursor_start"), run.dt_("cursor_terminus"), float(z["dt_s"]))
+    for k, st in enumerate(steps):
+        cur = st.cursor_off
+        active = (rel >= cur) & (rel - L <= cur) & alive
+        h = run.met.index(st.hour)
+        if h not in windows:
+            windows.clear()
+            windows[h] = hourly_window(run, h)
+        win = windows[h]
+        particles, state = scheme.step(particles, state, win, st.alpha, st.delta, active, None)
+        if win.metadata.time_start != last_bracket:
+            if conv is not None:
+                cur_step["k"] = k
+                particles, _ = conv.maybe_convect(particles, {}, win, t_alpha=st.alpha, dt_seconds=st.delta,
+                                                  active_mask=active, engine=None)
+            last_bracket = win.metadata.time_start
+        t_idx = ((wend - cur).clamp_(min=0.0) / 3600.0).floor().to(torch.int64)
+        if gridder.n_t == 1:
+            t_idx.clamp_(max=0)
+        gridder.accumulate(particles[:, :3], active, particles[:, 3], t_idx, ridx, st.delta)
+        lon, lat, zz = particles[:, 0], particles[:, 1], particles[:, 2]
+        within = (lon >= dl0) & (lon <= dl1) & (lat >= da0) & (lat <= da1) & (zz <= alt)
+        newly = active & ~within
+        alive = alive & ~newly
+        esc.append(int(newly.sum()))
+        act.append(int(active.sum()))
+    torch.cuda.synchronize()
+    return particles.T.cpu().numpy(), alive.cpu().numpy(), gridder.tensor.cpu().numpy(), np.array(esc), \
+        np.array(act), scheme.device_status
