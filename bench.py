@@ -60,6 +60,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
+    ap.add_argument("--workload", default="single-site", choices=["single-site", "multisite"],
+                    help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints")
+    ap.add_argument("--sites", type=int, default=56)
+    ap.add_argument("--release-times", type=int, default=48)
+    ap.add_argument("--days", type=float, default=5.0)
     return ap.parse_args()
 
 
@@ -276,8 +281,113 @@ def run_reference(args) -> None:
 # ---------------------------------------------------------------------------
 
 
+def multisite_workload(args, rank: int = 0):
+    """56 sites x 48 hourly 1 h releases, particle counts log-uniform in [2e3, 2e4]
+    (~2e7 in all), heights U(10, 300) m, 5 days backward at dt = 30 s, a 120-bin
+    time_ago footprint per release kept as two live slices (ring)."""
+    import dataclasses
+
+    from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.synthetic import config_met_spec
+
+    rng = np.random.default_rng(20261206 + rank)
+    n_sites, n_times = args.sites, args.release_times
+    length_s = args.days * 86400.0
+    base = config_met_spec(1)
+    t_rel0 = base.start_time + timedelta(hours=int(np.ceil(length_s / 3600.0)) + 1)
+    n_snap = int(np.ceil(length_s / 3600.0)) + n_times + 3
+    spec = dataclasses.replace(base, n_snapshots=n_snap, seed=20261206 + rank)
+    sites = np.stack([rng.uniform(-50.0, 30.0, n_sites), rng.uniform(20.0, 70.0, n_sites)], axis=1)
+    counts, heights, parts, rel_off, win_end, ridx = [], [], [], [], [], []
+    r = 0
+    for k in range(n_times - 1, -1, -1):  # latest releases first: they activate first walking backward
+        for s_i in range(n_sites):
+            n = int(np.exp(rng.uniform(np.log(2000.0), np.log(20000.0))))
+            h = rng.uniform(10.0, 300.0)
+            off = k * 3600.0
+            parts.append(np.stack([np.full(n, sites[s_i, 0]), np.full(n, sites[s_i, 1]), np.full(n, h),
+                                   np.full(n, 1.0 / n)], axis=1))
+            rel_off.append(off + rng.uniform(0.0, 3600.0, n))
+            win_end.append(np.full(n, off + 3600.0))
+            ridx.append(np.full(n, r))
+            counts.append(n)
+            r += 1
+    cfg = dict(
+        spec=spec, particles=np.concatenate(parts).astype(np.float32),
+        rel_off=np.concatenate(rel_off).astype(np.float32), win_end=np.concatenate(win_end).astype(np.float32),
+        ridx=np.concatenate(ridx).astype(np.int32), counts=np.array(counts), n_releases=r,
+        batch_start=t_rel0, cursor_start=t_rel0 + timedelta(hours=n_times),
+        terminus=t_rel0 + timedelta(hours=1) - timedelta(seconds=length_s), length_s=length_s,
+        hanna=HannaConfig(meander_enabled=True, max_substeps=6), emanuel=EmanuelConfig(),
+        footprint=FootprintSpec((-60.125, 40.125), (9.875, 80.125), 401, 281, (0.0, 100.0),
+                                int(np.ceil(length_s / 3600.0)), r, ring=2),
+        domain=DomainSpec((-60.0, 40.0), (10.0, 80.0), 20000.0),
+    )
+    return cfg
+
+
+def run_multisite(args) -> None:
+    """The batched multi-release job: every release in one particle batch, one fused
+    launch per met window, completed time_ago slices streamed to pinned host memory."""
+    import torch
+
+    from glide_b200.runtime import BatchRunner, ParticleState
+    from glide_b200.synthetic import SyntheticMet
+    from glide_b200.window import grid_from_synthetic, window_from_synthetic
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = multisite_workload(args)
+    syn = SyntheticMet(cfg["spec"], device=dev)
+    grid = grid_from_synthetic(syn).to_device(dev)
+    stream = torch.cuda.current_stream()
+    fp = cfg["footprint"]
+    slice_bytes = (len(fp.z_edges) - 1) * fp.n_y * fp.n_x * 4
+    staging = torch.empty(fp.n_releases * slice_bytes // 4, dtype=torch.float32).pin_memory()
+    totals = torch.zeros(fp.n_releases, fp.n_time_bins, dtype=torch.float64, device=dev)
+    moved = {"bytes": 0}
+
+    def sink(r_idx, b_idx, slices):
+        k = slices.shape[0]
+        staging[: k * slice_bytes // 4].view(k, -1).copy_(slices.view(k, -1), non_blocking=True)
+        moved["bytes"] += k * slice_bytes
+        totals[r_idx, b_idx] += slices.view(k, -1).sum(dim=1, dtype=torch.float64)
+
+    runner = BatchRunner(grid=grid, window_provider=lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid),
+                         hanna=cfg["hanna"], footprint=fp, domain=cfg["domain"], emanuel=cfg["emanuel"],
+                         met_dtype=args.met, device=dev, seed=77, footprint_sink=sink)
+    state = ParticleState.from_particles(cfg["particles"], cfg["rel_off"], cfg["win_end"], cfg["ridx"], dev)
+    run = runner.start(state, batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"],
+                       cursor_terminus=cfg["terminus"], sim_length_s=cfg["length_s"], dt_seconds=DT_S)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t_wall = time.perf_counter()
+    with ClockSampler(0) as clocks:
+        e0.record(stream)
+        run.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    t = e0.elapsed_time(e1) / 1e3
+    act = run.act[: len(run.steps)].cpu().numpy().astype(np.int64)
+    active_ps = int(act.sum())
+    n_total = int(cfg["particles"].shape[0])
+    line = {"metric": "active particle-steps/s", "value": active_ps / t, "unit": "particle-steps/s",
+            "footprints_per_s": cfg["n_releases"] / t, "n_gpus": 1, "workload": "multisite",
+            "releases": cfg["n_releases"], "particles": n_total, "outer_steps": len(run.steps),
+            "windows": len(run.windows), "active_particle_steps": active_ps,
+            "buffer_particle_steps_per_s": n_total * len(run.steps) / t, "device_s": t, "wall_s": wall,
+            "dtype": args.met, "footprint_d2h_bytes": moved["bytes"], "status": int(run.status.item()),
+            "footprint_total": float(totals.sum().item()), "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
+    if args.workload == "multisite":
+        run_multisite(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

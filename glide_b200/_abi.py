@@ -43,7 +43,7 @@ class StepSched(C.Structure):
 class FootprintGrid(C.Structure):
     _fields_ = [("lon_min", C.c_double), ("lon_max", C.c_double), ("lat_min", C.c_double), ("lat_max", C.c_double),
                 ("n_releases", C.c_int32), ("n_time_bins", C.c_int32), ("n_z", C.c_int32), ("n_y", C.c_int32),
-                ("n_x", C.c_int32), ("z_edges", vp)]
+                ("n_x", C.c_int32), ("z_edges", vp), ("ring", C.c_int32)]
 
 
 class StepArgs(C.Structure):

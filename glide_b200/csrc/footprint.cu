@@ -67,6 +67,8 @@ extern "C" glide_status glide_footprint_accumulate(int64_t n, const float* lon, 
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: NULL pointer");
     if (g->n_releases < 1 || g->n_time_bins < 1 || g->n_z < 1 || g->n_y < 1 || g->n_x < 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: empty grid");
+    if (g->ring != 0)
+        return set_error(GLIDE_ERR_UNSUPPORTED, "glide_footprint_accumulate: ring layout is only for glide_step");
     if (pos_stride < 1 || weight_stride < 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: stride < 1");
     FpDev d;

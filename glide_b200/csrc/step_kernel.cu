@@ -49,7 +49,7 @@ struct StepDev {
     const float* noise_sub; const float* noise_mea; uint32_t seed_lo, seed_hi;
     float* fp;
     float fp_lon0, fp_lon_span, fp_lat0, fp_lat_span;
-    int fp_R, fp_T, fp_Z, fp_Y, fp_X;
+    int fp_R, fp_T, fp_Z, fp_Y, fp_X, fp_ring;
     const float* fp_edges;
     float dom_lon0, dom_lon1, dom_lat0, dom_lat1, dom_alt;
     int32_t* esc; int32_t* act;
@@ -485,7 +485,10 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
                 valid = (rid >= 0) && (rid < p.fp_R) && (xf >= 0.0f) && (xf < (float)p.fp_X) && (yf >= 0.0f) &&
                         (yf < (float)p.fp_Y) && (zb >= 0) && (zb < p.fp_Z) && (tb >= 0) && (tb < p.fp_T);
                 if (valid) {
-                    flat = ((((int64_t)rid * p.fp_T + tb) * p.fp_Z + zb) * p.fp_Y + (int64_t)yf) * p.fp_X + (int64_t)xf;
+                    const int slot = p.fp_ring > 0 ? tb % p.fp_ring : tb;
+                    const int n_slot = p.fp_ring > 0 ? p.fp_ring : p.fp_T;
+                    flat = ((((int64_t)rid * n_slot + slot) * p.fp_Z + zb) * p.fp_Y + (int64_t)yf) * p.fp_X +
+                           (int64_t)xf;
                 }
             }
             const unsigned vmask = __ballot_sync(0xffffffffu, valid);
@@ -571,7 +574,7 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
     if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
-                         a->fp.n_time_bins < 1 || a->fp.n_releases < 1))
+                         a->fp.n_time_bins < 1 || a->fp.n_releases < 1 || a->fp.ring < 0))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: invalid footprint grid");
     if (a->post_begin < a->n_steps && !a->active_mask && a->footprint && !a->win_end_off)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: footprint needs win_end_off");
@@ -603,6 +606,7 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.fp_lat_span = (float)fmax(1e-6, a->fp.lat_max - a->fp.lat_min);
     d.fp_R = a->fp.n_releases; d.fp_T = a->fp.n_time_bins; d.fp_Z = a->fp.n_z; d.fp_Y = a->fp.n_y;
     d.fp_X = a->fp.n_x; d.fp_edges = a->fp.z_edges;
+    d.fp_ring = a->fp.ring;
     d.dom_lon0 = (float)a->dom_lon_min; d.dom_lon1 = (float)a->dom_lon_max;
     d.dom_lat0 = (float)a->dom_lat_min; d.dom_lat1 = (float)a->dom_lat_max;
     d.dom_alt = (float)a->dom_alt_max;

@@ -68,10 +68,16 @@ class FootprintSpec:
     z_edges: tuple[float, ...]
     n_time_bins: int
     n_releases: int = 1
+    ring: int = 0  # > 0: keep only `ring` live time-ago slices per release, flushed as bins complete
 
     @property
     def shape(self) -> tuple[int, int, int, int, int]:
         return (self.n_releases, self.n_time_bins, len(self.z_edges) - 1, self.n_y, self.n_x)
+
+    @property
+    def device_shape(self) -> tuple[int, int, int, int, int]:
+        t = self.ring if self.ring > 0 else self.n_time_bins
+        return (self.n_releases, t, len(self.z_edges) - 1, self.n_y, self.n_x)
 
 
 @dataclass(frozen=True)
@@ -189,7 +195,32 @@ class BatchRun:
         self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.footprint = torch.zeros(runner.footprint.shape, dtype=torch.float32, device=dev)
+        fp = runner.footprint
+        self.footprint = torch.zeros(fp.device_shape, dtype=torch.float32, device=dev)
+        self.footprint_out = None
+        self.sink = runner.footprint_sink
+        if fp.ring > 0:
+            if fp.n_time_bins == 1:
+                raise ValueError("ring footprints need n_time_bins > 1 (a single bin is already one slice)")
+            # each release's particles share one window end (release_generator.py:312-314): one bin per step
+            ends = np.full(fp.n_releases, np.nan, dtype=np.float32)
+            r_host = state.release_idx.cpu().numpy()
+            w_host = state.win_end_off.cpu().numpy()
+            for r in np.unique(r_host):
+                vals = np.unique(w_host[r_host == r])
+                if vals.size != 1:
+                    raise ValueError(f"ring footprints need one window end per release (release {r} has {vals.size})")
+                if 0 <= r < fp.n_releases:
+                    ends[r] = vals[0]
+            self.release_end = ends
+            if self.sink is None:
+                self.footprint_out = torch.zeros(fp.shape, dtype=torch.float32, device=dev)
+                out = self.footprint_out
+
+                def sink(r_idx, b_idx, slices):
+                    out[r_idx, b_idx] += slices
+
+                self.sink = sink
         self.z_edges = torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32), device=dev)
         # windows = runs of consecutive steps with the same hour
         self.windows: list[tuple[int, int]] = []
@@ -239,7 +270,7 @@ class BatchRun:
         fp = r.footprint
         a.fp = _abi.FootprintGrid(fp.lon_bounds[0], fp.lon_bounds[1], fp.lat_bounds[0], fp.lat_bounds[1],
                                   fp.n_releases, fp.n_time_bins, len(fp.z_edges) - 1, fp.n_y, fp.n_x,
-                                  self.z_edges.data_ptr())
+                                  self.z_edges.data_ptr(), fp.ring)
         d = r.domain
         a.dom_lon_min, a.dom_lon_max = d.lon_bounds
         a.dom_lat_min, a.dom_lat_max = d.lat_bounds
@@ -281,12 +312,44 @@ class BatchRun:
         else:
             a = self._step_args(packed, j0, n, 0, 0, noise)
             _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+        if r.footprint.ring > 0:
+            self._flush_completed_bins(j0, j1)
         prov = r.window_provider
         if hasattr(prov, "window_done"):  # streaming provider: release this window, prefetch the next
             prov.window_done(first.hour)
             if not self.done:
                 prov.prefetch(self.steps[self.windows[self.next_window][0]].hour)
         return True
+
+    def _bins(self, j: int) -> np.ndarray:
+        """Time-ago bin of every release at step j (main.py:1459-1465, float32)."""
+        el = np.maximum(self.release_end - np.float32(self.steps[j].cursor_off), np.float32(0.0))
+        with np.errstate(invalid="ignore"):
+            return np.floor(el / np.float32(3600.0))
+
+    def _flush_completed_bins(self, j0: int, j1: int) -> None:
+        """After window [j0, j1): hand every bin no later step can reach to the sink and
+        clear its ring slot. Bins advance with the cursor, so a bin is complete once the
+        next step's bin is past it (or the batch ends)."""
+        fp = self.r.footprint
+        lo = self._bins(j0)
+        hi = self._bins(j1 - 1)
+        nxt = self._bins(j1) if j1 < len(self.steps) else np.full_like(hi, np.inf)
+        r_idx, b_idx = [], []
+        for r in np.nonzero(np.isfinite(lo))[0]:
+            for b in range(int(lo[r]), int(hi[r]) + 1):
+                if b < nxt[r] and 0 <= b < fp.n_time_bins:
+                    r_idx.append(int(r))
+                    b_idx.append(b)
+        if not r_idx:
+            return
+        dev = self.footprint.device
+        ri = torch.as_tensor(r_idx, dtype=torch.int64, device=dev)
+        bi = torch.as_tensor(b_idx, dtype=torch.int64, device=dev)
+        si = bi % fp.ring
+        slices = self.footprint[ri, si]
+        self.sink(ri, bi, slices)
+        self.footprint[ri, si] = 0.0
 
     def _convect(self, wf: WindowFields, j: int, stream) -> None:
         r, s, e = self.r, self.state, self.r.emanuel
@@ -331,7 +394,8 @@ class BatchRun:
     def finish(self) -> BatchOutput:
         n = len(self.steps)
         status = int(self.status.item())
-        return BatchOutput(self.state, self.footprint, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
+        fp = self.footprint if self.r.footprint.ring == 0 else self.footprint_out
+        return BatchOutput(self.state, fp, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
                            self.conv_log, status)
 
 
@@ -348,7 +412,8 @@ class BatchRunner:
     def __init__(self, *, grid: GridInfo, window_provider: Callable[[datetime], WindowFields], hanna: HannaConfig,
                  footprint: FootprintSpec, domain: DomainSpec, emanuel: EmanuelConfig | None = None,
                  met_dtype: str = "f32", device="cuda", seed: int = 0,
-                 noise_provider: Callable | None = None, conv_uniform_provider: Callable | None = None) -> None:
+                 noise_provider: Callable | None = None, conv_uniform_provider: Callable | None = None,
+                 footprint_sink: Callable | None = None) -> None:
         self.device = torch.device(device)
         self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
         self.window_provider = window_provider
@@ -360,6 +425,7 @@ class BatchRunner:
         self.seed = int(seed)
         self.noise_provider = noise_provider
         self.conv_uniform_provider = conv_uniform_provider
+        self.footprint_sink = footprint_sink  # ring mode: sink(release_idx, bin_idx, slices [k, Zb, Y, X])
         self._packed = PackedWindow(self.grid, met_dtype, self.device)
 
     def packed_for(self, wf: WindowFields, stream=None) -> PackedWindow:

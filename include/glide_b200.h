@@ -94,6 +94,10 @@ typedef struct glide_footprint_grid {
     double lon_min, lon_max, lat_min, lat_max;
     int32_t n_releases, n_time_bins, n_z, n_y, n_x;
     const float* z_edges;        /* device [n_z + 1], ascending */
+    /* 0: dense [n_releases][n_time_bins][n_z][n_y][n_x]. k > 0: ring of k live
+     * time-ago slices per release, [n_releases][k][n_z][n_y][n_x], bin t stored in
+     * slot t % k; the caller flushes a slot once its bin can no longer be reached. */
+    int32_t ring;
 } glide_footprint_grid;
 
 typedef struct glide_step_args {

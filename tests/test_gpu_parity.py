@@ -238,3 +238,25 @@ def test_schemes_are_registered():
         get_scheme("nope")
     with pytest.raises(ValueError):
         get_scheme("hanna_1982_b200", max_substeps=0)
+
+
+def test_ring_footprint_matches_dense(cuda_device):
+    """Two live time-ago slices per release, flushed as bins complete, give the dense
+    (release x time_ago) footprint."""
+    import dataclasses
+
+    run = load_run("run_small")
+    out_dense = run_gpu(run, cuda_device)
+    r = runner_for(run, cuda_device)
+    r.footprint = dataclasses.replace(r.footprint, ring=2)
+    z = run.z
+    st = state_from(z["particles0"], z["rel_off"], z["win_end_off"], z["release_idx"], cuda_device)
+    out_ring = r.start(st, batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
+                       cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]),
+                       dt_seconds=float(z["dt_s"])).run()
+    torch.cuda.synchronize()
+    a = out_dense.footprint.cpu().numpy()
+    b = out_ring.footprint.cpu().numpy()
+    assert a.shape == b.shape and a.sum() > 0
+    np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-7)
+    assert r.footprint.device_shape[1] == 2
