@@ -60,8 +60,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
-    ap.add_argument("--workload", default="single-site", choices=["single-site", "multisite"],
-                    help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints")
+    ap.add_argument("--workload", default="single-site", choices=["single-site", "multisite", "serving"],
+                    help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints; "
+                         "serving: Poisson stream of footprint requests through FootprintServer")
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--rate", type=float, default=5.0)
+    ap.add_argument("--max-active", type=int, default=64)
+    ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
@@ -383,10 +388,74 @@ def run_multisite(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args) -> None:
+    """Poisson stream (default 5 requests/s, 2,000 requests) of footprint requests:
+    site among 56, release time uniform in 48 h, particles log-uniform in
+    [1e3, 5e4], backward duration uniform in [6, 120] h, dt 30 s, BF16 met with all
+    169 windows resident; 60 GB budget for particle state and footprints. Reports
+    throughput and p50/p90/p99 end-to-end latency, and the same requests run one at a
+    time (no overlap) for comparison."""
+    import dataclasses
+
+    import torch
+
+    from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.serving import FootprintServer, poisson_requests
+    from glide_b200.synthetic import SyntheticMet, config_met_spec
+    from glide_b200.window import grid_from_synthetic, window_from_synthetic
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    base = config_met_spec(1)
+    spec = dataclasses.replace(base, n_snapshots=171, seed=20261207)
+    syn = SyntheticMet(spec, device=dev)
+    grid = grid_from_synthetic(syn).to_device(dev)
+    t_rel0 = syn.times[0] + timedelta(hours=121)
+    rng = np.random.default_rng(20261207)
+    sites = np.stack([rng.uniform(-50.0, 30.0, 56), rng.uniform(20.0, 70.0, 56)], axis=1)
+    reqs = poisson_requests(args.requests, args.rate, sites, t_rel0, 48.0, seed=20261207)
+    kw = dict(grid=grid, met_provider=lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid),
+              horizon_start=syn.times[0], horizon_end=syn.times[-1],
+              hanna=HannaConfig(meander_enabled=True, max_substeps=6), emanuel=EmanuelConfig(),
+              footprint=FootprintSpec((-60.125, 40.125), (9.875, 80.125), 401, 281, (0.0, 100.0), 1),
+              domain=DomainSpec((-60.0, 40.0), (10.0, 80.0), 20000.0), met_dtype=args.met if args.met != "f32"
+              else "bf16", device=dev, hbm_budget_bytes=60e9)
+    t_pack = time.perf_counter()
+    server = FootprintServer(max_active=args.max_active, n_streams=16, **kw)
+    t_pack = time.perf_counter() - t_pack
+    with ClockSampler(0) as clocks:
+        t = time.perf_counter()
+        res = server.serve(reqs, realtime=True)
+        wall = time.perf_counter() - t
+    lat = np.array([r.latency_s for r in res])
+    aps = sum(r.active_particle_steps for r in res)
+    line = {"metric": "footprints/s", "value": len(res) / wall, "unit": "footprints/s", "workload": "serving",
+            "requests": len(res), "rate_per_s": args.rate, "wall_s": wall,
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                          "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "active_particle_steps_per_s": aps / wall, "peak_active": server.stats.peak_active,
+            "peak_state_bytes": server.stats.peak_bytes, "resident_packed_bytes": server.resident.nbytes,
+            "pack_s": t_pack, "dtype": kw["met_dtype"], "clocks": clocks.summary()}
+    if not args.no_sequential:
+        seq = FootprintServer(max_active=1, n_streams=1, **kw)
+        t = time.perf_counter()
+        sres = seq.serve([dataclasses.replace(r) for r in reqs], realtime=False)
+        swall = time.perf_counter() - t
+        service = np.array([r.finished_s - r.admitted_s for r in sres])
+        line["one_at_a_time"] = {"footprints_per_s": len(sres) / swall, "wall_s": swall,
+                                 "service_s_p50": float(np.percentile(service, 50)),
+                                 "service_s_p99": float(np.percentile(service, 99)),
+                                 "active_particle_steps_per_s": sum(r.active_particle_steps for r in sres) / swall}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.workload == "multisite":
         run_multisite(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

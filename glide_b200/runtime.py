@@ -413,7 +413,7 @@ class BatchRunner:
                  footprint: FootprintSpec, domain: DomainSpec, emanuel: EmanuelConfig | None = None,
                  met_dtype: str = "f32", device="cuda", seed: int = 0,
                  noise_provider: Callable | None = None, conv_uniform_provider: Callable | None = None,
-                 footprint_sink: Callable | None = None) -> None:
+                 footprint_sink: Callable | None = None, packed_provider: Callable | None = None) -> None:
         self.device = torch.device(device)
         self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
         self.window_provider = window_provider
@@ -426,9 +426,13 @@ class BatchRunner:
         self.noise_provider = noise_provider
         self.conv_uniform_provider = conv_uniform_provider
         self.footprint_sink = footprint_sink  # ring mode: sink(release_idx, bin_idx, slices [k, Zb, Y, X])
-        self._packed = PackedWindow(self.grid, met_dtype, self.device)
+        # packed_provider(hour) -> PackedWindow: windows packed elsewhere and shared (read-only)
+        self.packed_provider = packed_provider
+        self._packed = None if packed_provider is not None else PackedWindow(self.grid, met_dtype, self.device)
 
     def packed_for(self, wf: WindowFields, stream=None) -> PackedWindow:
+        if self.packed_provider is not None:
+            return self.packed_provider(wf.time_start)
         if self._packed.key != wf.time_start:
             self._packed.pack(wf, meander_coefficient=self.hanna.meander_coefficient,
                               meander_radius=self.hanna.meander_stencil_radius,
