@@ -53,14 +53,17 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"],
+                    help="reference: the reference algorithm on the host cores (oracle port); reference-gpu: "
+                         "the reference's own torch.compile CUDA-graph step path installed in baseline/_ref")
     ap.add_argument("--met", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
-    ap.add_argument("--workload", default="single-site", choices=["single-site", "multisite", "serving"],
+    ap.add_argument("--workload", default="single-site",
+                    choices=["single-site", "multisite", "serving", "precision"],
                     help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints; "
                          "serving: Poisson stream of footprint requests through FootprintServer")
     ap.add_argument("--requests", type=int, default=2000)
@@ -449,8 +452,225 @@ def run_serving(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args) -> None:
+    """The reference's own GPU path on this workload: its HannaScheme static step core
+    compiled with torch.compile(mode="reduce-overhead") (GLIDE_COMPILE=1), its Emanuel
+    convection, FootprintGridder and escape kill, driven step by step as its cursor
+    loop does (main.py:1382-1477), with its own RNG. Needs the reference installed in
+    baseline/_ref (pip install --no-deps --target baseline/_ref <reference>). The hot
+    path imports xarray only for annotations; a two-class stand-in module is supplied."""
+    import tempfile
+
+    os.environ["GLIDE_COMPILE"] = "1"
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "lpdm").is_dir():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "reference not installed in baseline/_ref"}))
+        return
+    stub = Path(tempfile.mkdtemp(prefix="glide_xr_"))
+    (stub / "xarray").mkdir()
+    (stub / "xarray" / "__init__.py").write_text("class Dataset:\n    pass\n\n\nclass DataArray:\n    pass\n")
+    sys.path.insert(0, str(ref))
+    sys.path.insert(0, str(stub))
+    from types import SimpleNamespace
+
+    import torch
+
+    import lpdm.convection.emanuel as em
+    import lpdm.footprint_gridder as fg
+    import lpdm.gpu_engine as ge
+    import lpdm.main as lm
+    import lpdm.met_reader as mr
+    import lpdm.turbulence.hanna as hn
+
+    from glide_b200.synthetic import SyntheticMet
+
+    n = args.particles
+    cfg = workload(n, 0, n_snapshots=max(5, args.snapshots if args.snapshots < 26 else 5))
+    dev = torch.device("cuda")
+    syn = SyntheticMet(cfg["spec"], device=dev)
+
+    def ref_window(h):
+        w = syn.window(h, device="cpu")
+        md = w.metadata
+        return mr.HourlyMetTensors(
+            hour_start=w.hour_start.contiguous(), hour_end=w.hour_end.contiguous(),
+            metadata=mr.MetFieldMetadata(lon=md.lon, lat=md.lat, level=md.level,
+                                         pressure_level_hpa=md.pressure_level_hpa, time_start=md.time_start,
+                                         time_end=md.time_end, variable_units=dict(md.variable_units)),
+            channel_names=w.channel_names, height_agl_m=w.height_agl_m.contiguous())
+
+    scheme = hn.HannaScheme(meander_enabled=True, max_substeps=6)
+    conv = em.EmanuelReducedConvection()
+    engine = ge.GPUEngine(device="cuda")
+    fp = cfg["footprint"]
+    gridder = fg.FootprintGridder(lon_bounds=fp.lon_bounds, lat_bounds=fp.lat_bounds, z_edges_m=fp.z_edges,
+                                  n_time_bins=fp.n_time_bins, n_y=fp.n_y, n_x=fp.n_x, n_releases=1, device=dev)
+    dom = cfg["domain"]
+    mcfg = SimpleNamespace(met_domain=SimpleNamespace(lon_bounds=dom.lon_bounds, lat_bounds=dom.lat_bounds,
+                                                      alt_max_m=dom.alt_max_m))
+    p = torch.as_tensor(cfg["particles"], device=dev)
+    rel = torch.as_tensor(cfg["rel_off"], device=dev)
+    wend = torch.as_tensor(cfg["win_end"], device=dev)
+    ridx = torch.zeros(n, dtype=torch.int64, device=dev)
+    state = scheme.initialize_state(n, device=dev, dtype=torch.float32)
+    alive = torch.ones(n, dtype=torch.bool, device=dev)
+    t_cursor, term = cfg["cursor_start"], cfg["terminus"]
+    bstart = cfg["batch_start"].timestamp()
+    windows: dict = {}
+    last = None
+    wcache: dict = {}
+    n_warm = 130  # the compile, the one-step first window and a full window
+    n_time = 240
+    for k in range(n_warm + n_time):
+        if k == n_warm:
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        delta = min(DT_S, (t_cursor - term).total_seconds())
+        cur = t_cursor.timestamp() - bstart
+        active = (rel >= cur) & (rel - SIM_LENGTH_S <= cur) & alive
+        h = syn.window_index(lm._hour_floor(t_cursor))
+        if h not in windows:
+            windows.clear()
+            windows[h] = ref_window(h)
+        win = windows[h]
+        alpha, _ = lm._advection_alpha_wind_mean(win, t_cursor, delta, dev, torch.float32, wcache)
+        p, state = scheme.step(particles=p, state=state, met_window=win, t_alpha=alpha, dt_seconds=delta,
+                               active_mask=active, engine=engine)
+        if win.metadata.time_start != last:
+            p, _ = conv.maybe_convect(particles=p, state={}, met_window=win, t_alpha=alpha, dt_seconds=delta,
+                                      active_mask=active, engine=engine)
+            last = win.metadata.time_start
+        t_idx = ((wend - cur).clamp_(min=0.0) / 3600.0).floor().to(torch.int64)
+        gridder.accumulate(particles=p[:, :3], active_mask=active, weights=p[:, 3], t_idx=t_idx, release_idx=ridx,
+                           dt_seconds=delta)
+        alive = alive & ~(active & ~lm._within_met_domain(p, mcfg))
+        t_cursor = t_cursor - timedelta(seconds=delta)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    value = n * n_time / t
+    print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+                      "steps": n_time, "warmup": n_warm, "ms_per_step": 1e3 * t / n_time, "higher_is_better": True,
+                      "dtype": "f32", "data": "synthetic", "graph_state": scheme._graph_compile_state,
+                      "config": {"workload": "single-site 24 h backward, 200k particles, 60x281x401 met, dt 30 s",
+                                 "step": "one outer step (the reference's graph replay + convection + gridder)"}}),
+          flush=True)
+
+
+def run_precision(args) -> None:
+    """Precision sweep on the single-site workload: met stored float32, bf16 and fp16
+    (interpolation and integration in float32, convective column in FP64) against
+    the FP64 oracle on the same met, the same injected noise and uniforms, for a
+    subsample of the release (``--particles``, default 2,000) over 24 h. Reports
+    trajectory drift at 1, 6 and 24 h, footprint relative L1 and peak-cell error, and
+    drop counts."""
+    import torch
+
+    from glide_b200.runtime import BatchRunner, ParticleState
+    from glide_b200.synthetic import SyntheticMet
+    from glide_b200.window import grid_from_synthetic, window_from_synthetic
+    from oracle.convection import EmanuelParams
+    from oracle.hanna import HannaParams, StepNoise
+    from oracle.runtime import DomainSpec, GridSpec, run_batch
+
+    n = args.particles if args.particles != N_PARTICLES else 2000
+    dev = torch.device("cuda", 0)
+    cfg = workload(n)
+    syn = SyntheticMet(cfg["spec"], device=dev)
+    grid = grid_from_synthetic(syn).to_device(dev)
+    ms = 6
+    seed, cseed = 424242, 515151
+
+    def step_noise(k):
+        rng = np.random.default_rng([seed, k])
+        return rng.standard_normal((ms, 3, n), dtype=np.float32), rng.standard_normal((2, n), dtype=np.float32)
+
+    def uniforms(k):
+        rng = np.random.default_rng([cseed, k])
+        return rng.random(n, dtype=np.float32), rng.random(n, dtype=np.float32)
+
+    def noise_provider(steps):
+        sub, mea = zip(*(step_noise(k) for k in steps))
+        return torch.from_numpy(np.stack(sub)).to(dev), torch.from_numpy(np.stack(mea)).to(dev)
+
+    def conv_provider(k):
+        return torch.from_numpy(np.stack(uniforms(k))).to(dev)
+
+    marks = {"1h": 1 + 120, "6h": 1 + 6 * 120, "24h": 2880}
+    results = {}
+    for mode in ("f32", "bf16", "f16"):
+        r = BatchRunner(grid=grid, window_provider=lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid),
+                        hanna=cfg["hanna"], footprint=cfg["footprint"], domain=cfg["domain"], emanuel=cfg["emanuel"],
+                        met_dtype=mode, device=dev, noise_provider=noise_provider, conv_uniform_provider=conv_provider)
+        st = ParticleState.from_particles(cfg["particles"], cfg["rel_off"], cfg["win_end"], cfg["ridx"], dev)
+        run = r.start(st, batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"],
+                      cursor_terminus=cfg["terminus"], sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S)
+        snaps = {}
+        while run.step_window():
+            done = run.windows[run.next_window - 1][1]
+            for name, k in marks.items():
+                if done == k:
+                    s = run.state
+                    snaps[name] = np.stack([s.lon.cpu().numpy(), s.lat.cpu().numpy(), s.z.cpu().numpy()])
+        out = run.finish()
+        results[mode] = dict(snaps=snaps, fp=out.footprint.cpu().numpy(), esc=int(out.escaped_per_step.sum()),
+                             status=out.status)
+    # FP64 oracle on the same met (copied from the device), noise and uniforms
+    cache = {}
+
+    def get_window(hk):
+        h = syn.window_index(hk)
+        if h not in cache:
+            cache.clear()
+            f0, f1 = syn.fields[h], syn.fields[h + 1]
+            w = {k: np.stack([f0[k].cpu().numpy(), f1[k].cpu().numpy()]) for k in f0}
+            w["height"] = syn.height_agl.cpu().numpy()
+            w.update(level=syn.levels, p_hpa=syn.pressure_level_hpa, lon=syn.lon, lat=syn.lat,
+                     time_start=syn.times[h], time_end=syn.times[h + 1])
+            cache[h] = w
+        return cache[h]
+
+    fp = cfg["footprint"]
+    dom = cfg["domain"]
+    t = time.perf_counter()
+    ora = run_batch(get_window=get_window, particles=cfg["particles"].T.copy(), rel_off=cfg["rel_off"],
+                    win_end_off=cfg["win_end"], release_idx=cfg["ridx"].astype(np.int64),
+                    batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"], cursor_terminus=cfg["terminus"],
+                    sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S, params=HannaParams(meander_enabled=True, max_substeps=ms),
+                    grid=GridSpec(fp.lon_bounds, fp.lat_bounds, fp.n_x, fp.n_y, fp.z_edges, fp.n_time_bins, 1),
+                    domain=DomainSpec(dom.lon_bounds, dom.lat_bounds, dom.alt_max_m),
+                    noise_fn=lambda k: StepNoise(*step_noise(k)), emanuel=EmanuelParams(),
+                    conv_uniforms_fn=uniforms, dtype=np.float64, conv_dtype=np.float64,
+                    snapshot_steps=tuple(marks.values()))
+    t_oracle = time.perf_counter() - t
+    ofp = ora.footprint
+    line = {"workload": "precision", "particles": n, "oracle": "FP64 numpy oracle", "oracle_s": t_oracle,
+            "oracle_escaped": int(sum(ora.escaped_per_step)), "modes": {}}
+    for mode, res in results.items():
+        d = {"status": res["status"], "escaped": res["esc"]}
+        for name, k in marks.items():
+            a, b = res["snaps"][name], ora.snapshots[k][:3]
+            dx = (a[0] - b[0]) * 111320.0 * np.cos(np.deg2rad(b[1]))
+            dy = (a[1] - b[1]) * 110540.0
+            d[f"rms_horizontal_m_{name}"] = float(np.sqrt(np.mean(dx * dx + dy * dy)))
+            d[f"rms_vertical_m_{name}"] = float(np.sqrt(np.mean((a[2] - b[2]) ** 2)))
+            d[f"median_rel_{name}"] = float(np.median(np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1)))
+        d["footprint_rel_l1"] = float(np.abs(res["fp"] - ofp).sum() / np.abs(ofp).sum())
+        d["footprint_peak_rel_err"] = float(abs(res["fp"].max() - ofp.max()) / ofp.max())
+        line["modes"][mode] = d
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
+    if args.workload == "precision":
+        run_precision(args)
+        return
+    if args.impl == "reference-gpu":
+        run_reference_gpu(args)
+        return
     if args.workload == "multisite":
         run_multisite(args)
         return

@@ -137,6 +137,7 @@ class BatchResult:
     active_per_step: list = field(default_factory=list)
     convection: list = field(default_factory=list)  # (window start, fires, n_moved)
     n_steps: int = 0
+    snapshots: dict = field(default_factory=dict)
 
 
 def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win_end_off, release_idx,
@@ -146,14 +147,16 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
               conv_uniforms_fn: Callable[[int], tuple[np.ndarray, np.ndarray]] | None = None,
               dtype=np.float32, conv_dtype=None, max_steps: int | None = None,
               init_state: dict | None = None, init_alive=None, step_offset: int = 0,
-              inputs_cache: dict | None = None, convect_first: bool = True) -> BatchResult:
+              inputs_cache: dict | None = None, convect_first: bool = True,
+              snapshot_steps: tuple = ()) -> BatchResult:
     """The static cursor loop of ``main._run`` for one batch (main.py:1382-1477).
 
     ``init_state`` / ``init_alive`` / ``step_offset`` resume a batch mid-way: the
     loop starts at ``cursor_start`` from that state and numbers its steps from
     ``step_offset`` (the noise rows). ``inputs_cache`` keeps the per-window support
     stacks across calls; ``convect_first=False`` treats the first window as already
-    convected (a resumed mid-window start)."""
+    convected (a resumed mid-window start). ``snapshot_steps``: step counts after
+    which the particles are recorded in ``BatchResult.snapshots``."""
     dt = dtype
     conv_dt = conv_dtype or dtype
     n = particles.shape[1]
@@ -206,6 +209,8 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
         res.active_per_step.append(int(active.sum()))
         t_cursor = t_cursor - timedelta(seconds=delta)
         step += 1
+        if step in snapshot_steps:
+            res.snapshots[step] = p.copy()
     res.particles, res.state, res.alive = p, state, alive
     res.footprint = fp.reshape(grid.shape)
     res.n_steps = step
