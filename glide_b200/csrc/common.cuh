@@ -114,8 +114,45 @@ __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
     return make_float2(r * c, r * s);
 }
 
-// Philox streams used by the kernels (third counter word).
-enum : uint32_t { STREAM_SUBSTEP = 0x10000u, STREAM_MEANDER = 0x20000u, STREAM_CONVECTION = 0x30000u };
+// Philox streams used by the kernels (fourth counter word).
+enum : uint32_t { STREAM_SUBSTEP = 0x10000u, STREAM_MEANDER = 0x20000u, STREAM_CONVECTION = 0x30000u,
+                  STREAM_STEP = 0x40000u };
+
+// Normal deviates of one particle-step: one Philox-4x32-10 block keyed by
+// (particle, step) seeds a SplitMix64 sequence (Steele, Lea & Flood, "Fast
+// splittable pseudorandom number generators", OOPSLA 2014: Weyl increment and
+// the published two-multiply finaliser), whose 64-bit outputs feed Box-Muller
+// pairs; the second deviate of a pair is kept for the next draw.
+struct StepNormals {
+    uint64_t s;
+    float spare;
+    bool has_spare;
+
+    __device__ __forceinline__ StepNormals(uint64_t particle, uint32_t step, uint32_t k0, uint32_t k1) {
+        const U4 r = philox4x32_10(U4{(uint32_t)particle, (uint32_t)(particle >> 32), step, STREAM_STEP}, k0, k1);
+        s = ((uint64_t)r.y << 32 | r.x) ^ (((uint64_t)r.w << 32 | r.z) * 0x9E3779B97F4A7C15ull);
+        has_spare = false;
+        spare = 0.0f;
+    }
+    __device__ __forceinline__ uint64_t next64() {
+        s += 0x9E3779B97F4A7C15ull;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    __device__ __forceinline__ float next() {
+        if (has_spare) {
+            has_spare = false;
+            return spare;
+        }
+        const uint64_t z = next64();
+        const float2 g = box_muller((uint32_t)z, (uint32_t)(z >> 32));
+        spare = g.y;
+        has_spare = true;
+        return g.x;
+    }
+};
 
 // ---------------------------------------------------------------------------
 // Grid normalisation (src/lpdm/gpu_engine.py:210-299) and torch grid_sample

@@ -9,8 +9,8 @@
 //   length / w* -> Hanna column turbulence at z_eval and z_eval +- 1 m (free
 //   troposphere override from the support bricks) -> well-mixed + density
 //   drift -> per-particle exact-OU substeps (clip, displacement, reflection)
-//   -> meander OU -> [post] time-ago bin, warp-aggregated footprint atomic,
-//   escape kill.
+//   -> meander OU -> [post] time-ago bin, footprint residence time (cached per
+//   particle, one atomic per change of cell), escape kill.
 //
 // Met is read from the packed per-window bricks (window_pack.cu): the wind
 // brick holds u, v, w of both snapshots in one 32-byte (float32) or 16-byte
@@ -275,6 +275,11 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
     const float L_sim = p.sim_length;
     const int ms = p.max_substeps;
     bool nonfinite = false;
+    // footprint cache: a particle stays in one output cell for many steps, so its
+    // residence time accumulates in a register and goes to global memory (one
+    // atomic) only when the cell (or time bin) changes, and at the end of the launch
+    int64_t fp_cell = -1;
+    float fp_acc = 0.0f;
 
     for (int j = 0; j < p.n_steps; ++j) {
         const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
@@ -410,6 +415,7 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
             const float rv = sqrtf(fmaxf(sv2 * (1.0f - av * av), 0.0f));
             const float rw = sqrtf(fmaxf(sw2 * (1.0f - aw * aw), 0.0f));
             const int64_t nn = p.n;
+            StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
             for (int it = 0; it < k; ++it) {
                 float eu, ev, ew;
                 if (p.noise_sub) {
@@ -418,11 +424,9 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
                     ev = __ldg(b + nn);
                     ew = __ldg(b + 2 * nn);
                 } else {
-                    const U4 r = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sc.step_index,
-                                                  STREAM_SUBSTEP + (uint32_t)it}, p.seed_lo, p.seed_hi);
-                    const float2 n01 = box_muller(r.x, r.y);
-                    const float2 n23 = box_muller(r.z, r.w);
-                    eu = n01.x; ev = n01.y; ew = n23.x;
+                    eu = rng.next();
+                    ev = rng.next();
+                    ew = rng.next();
                 }
                 const float factor = 1.0f + (wp * wp) / sw_sq;
                 const float drift_w = factor * half_bwd + dens_bwd;
@@ -451,10 +455,8 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
                     e0 = __ldg(b);
                     e1 = __ldg(b + nn);
                 } else {
-                    const U4 r = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sc.step_index,
-                                                  STREAM_MEANDER}, p.seed_lo, p.seed_hi);
-                    const float2 n01 = box_muller(r.x, r.y);
-                    e0 = n01.x; e1 = n01.y;
+                    e0 = rng.next();
+                    e1 = rng.next();
                 }
                 const float am = expf(-delta / p.meander_T);
                 const float one_m = 1.0f - am * am;
@@ -491,19 +493,12 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
                            (int64_t)xf;
                 }
             }
-            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-            if (valid) {
-                // warp-aggregated atomic: lanes hitting the same cell sum by shuffles, one atomic per cell
-                const float w_eff = wgt * sc.delta;
-                const unsigned peers = __match_any_sync(vmask, (unsigned long long)flat);
-                float sum = 0.0f;
-                unsigned m = peers;
-                while (m) {
-                    const int src = __ffs(m) - 1;
-                    m &= m - 1;
-                    sum += __shfl_sync(peers, w_eff, src);
-                }
-                if (lane == __ffs(peers) - 1) atomicAdd(p.fp + flat, sum);
+            if (valid && flat == fp_cell) {
+                fp_acc += wgt * sc.delta;
+            } else {
+                if (fp_cell >= 0) atomicAdd(p.fp + fp_cell, fp_acc);
+                fp_cell = valid ? flat : -1;
+                fp_acc = valid ? wgt * sc.delta : 0.0f;
             }
             // --- escape kill (main.py:690-711, 1475-1477)
             bool escaped = false;
@@ -522,6 +517,7 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
         }
     }
 
+    if (fp_cell >= 0) atomicAdd(p.fp + fp_cell, fp_acc);
     if (have) {
         p.lon[i * p.ps] = lon;
         p.lat[i * p.ps] = lat;
