@@ -96,7 +96,16 @@ def _c0_spec(seed: int) -> SyntheticMetSpec:
                             seed=seed, start_time=datetime(2026, 1, 14, 23, tzinfo=UTC))
 
 
-def oracle_kwargs(run: GoldenRun, dtype=np.float32, conv_dtype=None):
+def flipped_levels(run: GoldenRun) -> GoldenRun:
+    """The same case with the met stored top-down (descending level order), as a
+    pressure-level reader would deliver it."""
+    m = run.met
+    fields = {k: (v[:, ::-1].copy() if v.ndim == 4 else v) for k, v in m.fields.items()}
+    met = MetArrays(fields, np.asarray(m.levels)[::-1].copy(), np.asarray(m.p_hpa)[::-1].copy(), m.lon, m.lat, m.t0)
+    return GoldenRun(run.name + "_desc", run.z, met)
+
+
+def oracle_kwargs(run: GoldenRun, dtype=np.float32, conv_dtype=None, hanna_kw: dict | None = None):
     """Keyword arguments of ``oracle.run_batch`` reproducing the golden batch."""
     from oracle.convection import EmanuelParams
     from oracle.hanna import HannaParams, StepNoise
@@ -119,7 +128,7 @@ def oracle_kwargs(run: GoldenRun, dtype=np.float32, conv_dtype=None):
         particles=z["particles0"], rel_off=z["rel_off"], win_end_off=z["win_end_off"], release_idx=z["release_idx"],
         batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
         cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]), dt_seconds=float(z["dt_s"]),
-        params=HannaParams(meander_enabled=bool(z["meander"]), max_substeps=ms),
+        params=HannaParams(meander_enabled=bool(z["meander"]), max_substeps=ms, **(hanna_kw or {})),
         grid=GridSpec(tuple(z["grid_lon"]), tuple(z["grid_lat"]), int(nxy[0]), int(nxy[1]), tuple(z["grid_z"]),
                       int(nxy[2]), n_rel),
         domain=DomainSpec(tuple(z["dom_lon"]), tuple(z["dom_lat"]), float(z["dom_alt"])),

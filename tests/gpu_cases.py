@@ -19,7 +19,7 @@ def grid_of(run: GoldenRun) -> GridInfo:
 
 
 def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool = True, met_dtype: str = "f32",
-               seed: int = 1234) -> BatchRunner:
+               seed: int = 1234, hanna_kw: dict | None = None) -> BatchRunner:
     z = run.z
     m = run.met
     grid = grid_of(run).to_device(device)
@@ -50,7 +50,7 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
     n_rel = int(z["release_idx"].max()) + 1
     return BatchRunner(
         grid=grid, window_provider=window_provider,
-        hanna=HannaConfig(meander_enabled=bool(z["meander"]), max_substeps=ms),
+        hanna=HannaConfig(meander_enabled=bool(z["meander"]), max_substeps=ms, **(hanna_kw or {})),
         footprint=FootprintSpec(tuple(z["grid_lon"]), tuple(z["grid_lat"]), int(nxy[0]), int(nxy[1]),
                                 tuple(float(e) for e in z["grid_z"]), int(nxy[2]), n_rel),
         domain=DomainSpec(tuple(z["dom_lon"]), tuple(z["dom_lat"]), float(z["dom_alt"])),

@@ -65,3 +65,13 @@ def test_invalid_arguments_are_rejected_without_a_device():
 def test_check_raises_with_text():
     with pytest.raises(_abi.GlideError, match="args is NULL"):
         _abi.check(_abi.lib.glide_step(None, None), "glide_step")
+
+
+def test_empty_launch_is_a_no_op_without_a_device():
+    a = _abi.StepArgs()
+    a.n = 0
+    a.n_steps = 1
+    assert _abi.lib.glide_step(C.byref(a), None) == 0
+    c = _abi.ConvectArgs()
+    c.n, c.nz, c.ny, c.nx = 0, 4, 2, 2
+    assert _abi.lib.glide_convect(C.byref(c), None) == 1  # met inputs are still required
