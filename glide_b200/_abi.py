@@ -86,6 +86,7 @@ SIGNATURES = {
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),
     "glide_convect": (C.c_int32, [C.POINTER(ConvectArgs), vp]),
     "glide_convect_noalloc": (C.c_int32, [C.POINTER(ConvectArgs), vp]),
+    "glide_convect_redistribute": (C.c_int32, [C.POINTER(ConvectArgs), vp]),
     "glide_convect_column_info": (C.c_int32, [vp, C.c_int32, vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                               C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                               C.POINTER(C.c_double)]),

@@ -362,6 +362,29 @@ extern "C" glide_status glide_convect(const glide_convect_args* a, void* stream)
     return check_launch("glide_convect");
 }
 
+extern "C" glide_status glide_convect_redistribute(const glide_convect_args* a, void* stream) {
+    if (!a) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: args is NULL");
+    if (a->nz < 2 || a->nz > 512) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: nz out of range");
+    if (a->n < 0) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: n < 0");
+    if (!a->scratch) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: scratch is NULL");
+    if (a->n > 0 && (!a->z || (!a->active_mask && !a->rel_off)))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: NULL particle input");
+    if (a->z_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: z_stride < 1");
+    if (((uintptr_t)a->scratch) & 7u)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_redistribute: scratch misaligned");
+    if (a->n == 0) return GLIDE_OK;
+    ConvDev d = {};
+    d.n = a->n; d.z = a->z; d.zs = a->z_stride;
+    d.rel_off = a->rel_off; d.alive = a->alive; d.active_mask = a->active_mask;
+    d.sim_length = a->sim_length_s; d.sched = a->sched;
+    d.nz = a->nz;
+    d.uniforms = a->uniforms; d.seed_lo = (uint32_t)a->seed; d.seed_hi = (uint32_t)(a->seed >> 32);
+    d.scratch = static_cast<double*>(a->scratch);
+    d.n_moved = a->n_moved;
+    redistribute_kernel<<<(unsigned)((a->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d);
+    return check_launch("glide_convect_redistribute");
+}
+
 extern "C" glide_status glide_convect_column_info(const void* scratch, int32_t nz, void* stream, int32_t* fires,
                                                   int32_t* i_lcl, int32_t* i_lnb, double* cape, double* dtv,
                                                   double* m_b) {

@@ -10,9 +10,13 @@ cursor offset) and then issues, per met window,
 * without convection: ONE ``glide_step`` launch covering every outer step of
   the window (physics + footprint + escape fused, state in registers);
 * with convection: ``glide_step`` for the physics of the window's first step,
-  ``glide_convect`` (column build + redistribution on the device), then one
+  ``glide_convect_redistribute`` against the window's column, then one
   ``glide_step`` that does the first step's footprint/escape and all remaining
   steps — the reference's step -> convection -> footprint -> kill order.
+
+The work that depends only on met (packing the bricks, building the convection
+column) is done for window k+1 on a side stream while window k's steps run,
+into the second of two brick / column slots.
 
 No launch synchronises with the host; per-step diagnostics (escaped and
 active counts) accumulate in device arrays read once per batch.
@@ -233,7 +237,18 @@ class BatchRun:
             k = e
         self.next_window = 0
         self.conv_log: list = []
-        self.conv_scratch = None
+        # per-window preparation, double-buffered when pipelined (bricks and column of
+        # window k+1 built on a side stream while window k's steps run)
+        self.pipelined = runner.pipeline and runner.packed_provider is None
+        self.prep_stream = torch.cuda.Stream(device=dev) if self.pipelined else None
+        self.prepared: dict = {}
+        self.slot_free: list = [None, None]
+        self.conv_scratch = []
+        if runner.emanuel is not None:
+            nb = C.c_size_t()
+            _abi.check(_abi.lib.glide_convect_scratch_bytes(runner.grid.shape[0], C.byref(nb)),
+                       "glide_convect_scratch_bytes")
+            self.conv_scratch = [torch.zeros(nb.value // 8, dtype=torch.float64, device=dev) for _ in range(2)]
 
     @property
     def done(self) -> bool:
@@ -280,18 +295,45 @@ class BatchRun:
         a.status = self.status.data_ptr()
         return a
 
+    def _prepare(self, k: int) -> None:
+        """Per-window work that depends only on met: fetch the window, pack its bricks
+        and build its convection column (``glide_convect`` with no particles), on the
+        prep stream (pipelined: overlapping the previous window's steps) or inline."""
+        r = self.r
+        j0 = self.windows[k][0]
+        first = self.steps[j0]
+        slot = k % 2 if self.pipelined else 0
+        prep_stream = self.prep_stream if self.pipelined else torch.cuda.current_stream(r.device)
+        with torch.cuda.stream(prep_stream):
+            if self.slot_free[slot] is not None:
+                prep_stream.wait_event(self.slot_free[slot])
+            wf = r.window_provider(first.hour)
+            if wf.time_start != first.hour:
+                raise ValueError(f"window provider returned {wf.time_start} for hour {first.hour}")
+            packed = r.packed_for(wf, prep_stream, slot=slot)
+            scratch = None
+            if r.emanuel is not None:
+                scratch = self.conv_scratch[slot]
+                a = self._convect_args(wf, j0, scratch, n_particles=0)
+                _abi.check(_abi.lib.glide_convect(C.byref(a), stream_handle(prep_stream)), "glide_convect")
+            ev = torch.cuda.Event()
+            ev.record(prep_stream)
+        self.prepared[k] = (wf, packed, scratch, ev)
+
     def step_window(self, stream=None) -> bool:
         """Issue the launches of the next met window; False when the batch is done."""
         if self.done:
             return False
         r = self.r
-        j0, j1 = self.windows[self.next_window]
+        k = self.next_window
+        j0, j1 = self.windows[k]
         self.next_window += 1
         first = self.steps[j0]
-        wf = r.window_provider(first.hour)
-        if wf.time_start != first.hour:
-            raise ValueError(f"window provider returned {wf.time_start} for hour {first.hour}")
-        packed = r.packed_for(wf, stream)
+        main = stream if stream is not None else torch.cuda.current_stream(r.device)
+        if k not in self.prepared:
+            self._prepare(k)
+        wf, packed, scratch, ready = self.prepared.pop(k)
+        main.wait_event(ready)
         noise = r.noise_provider(list(range(j0, j1))) if r.noise_provider is not None else None
         if noise is not None:  # the kernel indexes these buffers: check their extents first
             sub, mea = noise
@@ -301,24 +343,30 @@ class BatchRun:
             if r.hanna.meander_enabled and (mea is None or tuple(mea.shape) != (j1 - j0, 2, self.state.n)
                                             or mea.dtype != torch.float32 or not mea.is_contiguous()):
                 raise ValueError("injected meander noise must be contiguous float32 (steps, 2, n)")
-        sh = stream_handle(stream)
+        sh = stream_handle(main)
         n = j1 - j0
-        if r.emanuel is not None:
-            a = self._step_args(packed, j0, 1, 0, 1, noise)
-            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
-            self._convect(wf, j0, stream)
-            a = self._step_args(packed, j0, n, 1, 0, noise)
-            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
-        else:
-            a = self._step_args(packed, j0, n, 0, 0, noise)
-            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
-        if r.footprint.ring > 0:
-            self._flush_completed_bins(j0, j1)
-        prov = r.window_provider
-        if hasattr(prov, "window_done"):  # streaming provider: release this window, prefetch the next
-            prov.window_done(first.hour)
-            if not self.done:
-                prov.prefetch(self.steps[self.windows[self.next_window][0]].hour)
+        with torch.cuda.stream(main):
+            if r.emanuel is not None:
+                a = self._step_args(packed, j0, 1, 0, 1, noise)
+                _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+                self._redistribute(wf, j0, scratch, main)
+                a = self._step_args(packed, j0, n, 1, 0, noise)
+                _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+            else:
+                a = self._step_args(packed, j0, n, 0, 0, noise)
+                _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+            done = torch.cuda.Event()
+            done.record(main)
+            self.slot_free[k % 2 if self.pipelined else 0] = done
+            if r.footprint.ring > 0:
+                self._flush_completed_bins(j0, j1)
+            prov = r.window_provider
+            if hasattr(prov, "window_done"):  # streaming provider: release this window, prefetch the next
+                prov.window_done(first.hour)
+                if not self.done:
+                    prov.prefetch(self.steps[self.windows[self.next_window][0]].hour)
+        if self.pipelined and not self.done:
+            self._prepare(self.next_window)  # overlaps this window's steps
         return True
 
     def _bins(self, j: int) -> np.ndarray:
@@ -351,17 +399,12 @@ class BatchRun:
         self.sink(ri, bi, slices)
         self.footprint[ri, si] = 0.0
 
-    def _convect(self, wf: WindowFields, j: int, stream) -> None:
+    def _convect_args(self, wf: WindowFields, j: int, scratch: torch.Tensor, n_particles: int) -> _abi.ConvectArgs:
         r, s, e = self.r, self.state, self.r.emanuel
         nz, ny, nx = r.grid.shape
-        if self.conv_scratch is None:
-            nb = C.c_size_t()
-            _abi.check(_abi.lib.glide_convect_scratch_bytes(nz, C.byref(nb)), "glide_convect_scratch_bytes")
-            self.conv_scratch = torch.zeros(nb.value // 8, dtype=torch.float64, device=r.device)
-        moved = torch.zeros(1, dtype=torch.int32, device=r.device)
         st = self.steps[j]
         a = _abi.ConvectArgs()
-        a.n = s.n
+        a.n = n_particles
         a.z, a.z_stride = s.z.data_ptr(), 1
         a.rel_off, a.alive, a.active_mask = s.rel_off.data_ptr(), s.alive.data_ptr(), None
         a.sim_length_s = self.sim_length_s
@@ -376,14 +419,22 @@ class BatchRun:
         a.alpha = st.alpha
         a.closure_c, a.trigger_dtv_k = e.closure_c, e.trigger_dtv_k
         a.min_cape_j_kg, a.min_cloud_depth_m = e.min_cape_j_kg, e.min_cloud_depth_m
+        a.seed = r.seed
+        a.scratch = scratch.data_ptr()
+        return a
+
+    def _redistribute(self, wf: WindowFields, j: int, scratch: torch.Tensor, stream) -> None:
+        """The window's convective redistribution against its prebuilt column
+        (emanuel.py:720-805)."""
+        r, s = self.r, self.state
+        moved = torch.zeros(1, dtype=torch.int32, device=r.device)
+        a = self._convect_args(wf, j, scratch, n_particles=s.n)
         u = r.conv_uniform_provider(j) if r.conv_uniform_provider is not None else None
         if u is not None and (tuple(u.shape) != (2, s.n) or u.dtype != torch.float32 or not u.is_contiguous()):
             raise ValueError(f"injected convection uniforms must be contiguous float32 (2, {s.n})")
         a.uniforms = None if u is None else u.data_ptr()
-        a.seed = r.seed
-        a.scratch = self.conv_scratch.data_ptr()
         a.n_moved = moved.data_ptr()
-        _abi.check(_abi.lib.glide_convect(C.byref(a), stream_handle(stream)), "glide_convect")
+        _abi.check(_abi.lib.glide_convect_redistribute(C.byref(a), stream_handle(stream)), "glide_convect_redistribute")
         self.conv_log.append((wf.time_start, moved))
 
     def run(self, stream=None) -> BatchOutput:
@@ -413,7 +464,8 @@ class BatchRunner:
                  footprint: FootprintSpec, domain: DomainSpec, emanuel: EmanuelConfig | None = None,
                  met_dtype: str = "f32", device="cuda", seed: int = 0,
                  noise_provider: Callable | None = None, conv_uniform_provider: Callable | None = None,
-                 footprint_sink: Callable | None = None, packed_provider: Callable | None = None) -> None:
+                 footprint_sink: Callable | None = None, packed_provider: Callable | None = None,
+                 pipeline: bool = True) -> None:
         self.device = torch.device(device)
         self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
         self.window_provider = window_provider
@@ -428,16 +480,22 @@ class BatchRunner:
         self.footprint_sink = footprint_sink  # ring mode: sink(release_idx, bin_idx, slices [k, Zb, Y, X])
         # packed_provider(hour) -> PackedWindow: windows packed elsewhere and shared (read-only)
         self.packed_provider = packed_provider
-        self._packed = None if packed_provider is not None else PackedWindow(self.grid, met_dtype, self.device)
+        self.pipeline = bool(pipeline)
+        self._slots: list[PackedWindow | None] = [None, None]
 
-    def packed_for(self, wf: WindowFields, stream=None) -> PackedWindow:
+    def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:
+        """The packed bricks of ``wf`` (packed into brick slot ``slot`` unless a
+        ``packed_provider`` serves prebuilt windows)."""
         if self.packed_provider is not None:
             return self.packed_provider(wf.time_start)
-        if self._packed.key != wf.time_start:
-            self._packed.pack(wf, meander_coefficient=self.hanna.meander_coefficient,
-                              meander_radius=self.hanna.meander_stencil_radius,
-                              build_meander=self.hanna.meander_enabled, stream=stream)
-        return self._packed
+        if self._slots[slot] is None:
+            self._slots[slot] = PackedWindow(self.grid, self.met_dtype, self.device)
+        pw = self._slots[slot]
+        if pw.key != wf.time_start:
+            pw.pack(wf, meander_coefficient=self.hanna.meander_coefficient,
+                    meander_radius=self.hanna.meander_stencil_radius, build_meander=self.hanna.meander_enabled,
+                    stream=stream)
+        return pw
 
     def start(self, state: ParticleState, *, batch_start: datetime, cursor_start: datetime,
               cursor_terminus: datetime, sim_length_s: float, dt_seconds: float,

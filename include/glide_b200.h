@@ -206,6 +206,13 @@ glide_status glide_footprint_accumulate(int64_t n, const float* lon, const float
 glide_status glide_convect_scratch_bytes(int32_t nz, size_t* bytes);
 glide_status glide_convect(const glide_convect_args* args, void* stream);
 
+/* The per-particle half of glide_convect (_redistribute_particles,
+ * src/lpdm/convection/emanuel.py:720-805) against a column already built in
+ * args->scratch by an earlier glide_convect on the same scratch (with n = 0 that
+ * call builds the column only). Lets a runtime build the next window's column
+ * ahead of time on another stream. */
+glide_status glide_convect_redistribute(const glide_convect_args* args, void* stream);
+
 /* Maximum number of met levels that glide_convect_noalloc accepts. */
 #define GLIDE_CONVECT_NOALLOC_MAX_NZ 128
 
