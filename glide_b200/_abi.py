@@ -58,7 +58,7 @@ class StepArgs(C.Structure):
                 ("noise_substep", vp), ("noise_meander", vp), ("seed", C.c_uint64), ("footprint", vp),
                 ("fp", FootprintGrid), ("dom_lon_min", C.c_double), ("dom_lon_max", C.c_double),
                 ("dom_lat_min", C.c_double), ("dom_lat_max", C.c_double), ("dom_alt_max", C.c_double),
-                ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp)]
+                ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32)]
 
 
 class ConvectArgs(C.Structure):
@@ -81,6 +81,8 @@ SIGNATURES = {
                                               C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "glide_window_pack": (C.c_int32, [C.POINTER(WindowDesc), vp]),
     "glide_step": (C.c_int32, [C.POINTER(StepArgs), vp]),
+    "glide_step_launch_variants": (C.c_int32, [C.POINTER(C.c_int32)]),
+    "glide_step_launch_variant_info": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "glide_footprint_accumulate": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_float,
                                                C.POINTER(FootprintGrid), vp, vp]),
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),

@@ -241,12 +241,16 @@ __device__ __forceinline__ float noise_or_philox(const StepDev& p, const float* 
     return base ? __ldg(base + idx) : philox;
 }
 
-#ifndef GLIDE_STEP_MIN_BLOCKS
-#define GLIDE_STEP_MIN_BLOCKS 6  // <= 80 registers: 24 warps per SM (measured +9 % over 114 registers)
-#endif
+// Launch shapes (threads per block, resident blocks per SM the register budget
+// is compiled for). Variant 0, 128 x 6 (<= 80 registers, 24 warps per SM), is
+// the measured default; the others exist for the autotuner: the best shape
+// depends on the particle count (wave quantisation of a batch across 148 SMs).
+struct LaunchShape { int threads, min_blocks; };
+constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
-template <typename T>
-__global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const StepDev p) {
+template <typename T, int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev p) {
     extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool have = i < p.n;
@@ -536,13 +540,25 @@ __global__ void __launch_bounds__(128, GLIDE_STEP_MIN_BLOCKS) step_kernel(const 
     }
 }
 
-template <typename T>
-static glide_status launch_step(const StepDev& d, cudaStream_t stream) {
-    const int threads = 128;
+template <typename T, int V>
+static void launch_shape(const StepDev& d, cudaStream_t stream, size_t smem) {
+    constexpr int threads = kShapes[V].threads;
     const int64_t blocks = (d.n + threads - 1) / threads;
+    step_kernel<T, threads, kShapes[V].min_blocks><<<(unsigned)blocks, threads, smem, stream>>>(d);
+}
+
+template <typename T>
+static glide_status launch_step(const StepDev& d, cudaStream_t stream, int variant) {
     const size_t smem = sizeof(int32_t) * 2 * (size_t)d.n_steps;
     if (smem > 48 * 1024) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large", d.n_steps);
-    step_kernel<T><<<(unsigned)blocks, threads, smem, stream>>>(d);
+    switch (variant) {
+        case 0: launch_shape<T, 0>(d, stream, smem); break;
+        case 1: launch_shape<T, 1>(d, stream, smem); break;
+        case 2: launch_shape<T, 2>(d, stream, smem); break;
+        case 3: launch_shape<T, 3>(d, stream, smem); break;
+        case 4: launch_shape<T, 4>(d, stream, smem); break;
+        default: return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", variant);
+    }
     return check_launch("glide_step");
 }
 
@@ -568,6 +584,8 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (a->grid.nz < 2 || a->grid.ny < 2 || a->grid.nx < 2)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: grid must be at least 2x2x2");
     if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
+    if (a->launch_variant < 0 || a->launch_variant >= kNumShapes)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", a->launch_variant);
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
     if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
                          a->fp.n_time_bins < 1 || a->fp.n_releases < 1 || a->fp.ring < 0))
@@ -610,9 +628,23 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.status = a->status;
     cudaStream_t s = (cudaStream_t)stream;
     switch (a->met_dtype) {
-        case GLIDE_MET_F32: return launch_step<float>(d, s);
-        case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s);
-        case GLIDE_MET_F16: return launch_step<__half>(d, s);
+        case GLIDE_MET_F32: return launch_step<float>(d, s, a->launch_variant);
+        case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s, a->launch_variant);
+        case GLIDE_MET_F16: return launch_step<__half>(d, s, a->launch_variant);
         default: return set_error(GLIDE_ERR_UNSUPPORTED, "glide_step: unknown met_dtype %d", a->met_dtype);
     }
+}
+
+extern "C" glide_status glide_step_launch_variants(int32_t* count) {
+    if (!count) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_launch_variants: count is NULL");
+    *count = kNumShapes;
+    return GLIDE_OK;
+}
+
+extern "C" glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t* min_blocks) {
+    if (v < 0 || v >= kNumShapes)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_launch_variant_info: variant %d out of range", v);
+    if (threads) *threads = kShapes[v].threads;
+    if (min_blocks) *min_blocks = kShapes[v].min_blocks;
+    return GLIDE_OK;
 }

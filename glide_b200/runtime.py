@@ -293,6 +293,7 @@ class BatchRun:
         a.escaped_per_step = self.esc.data_ptr() + 4 * j0
         a.active_per_step = self.act.data_ptr() + 4 * j0
         a.status = self.status.data_ptr()
+        a.launch_variant = r.launch_variant
         return a
 
     def _prepare(self, k: int) -> None:
@@ -481,6 +482,7 @@ class BatchRunner:
         # packed_provider(hour) -> PackedWindow: windows packed elsewhere and shared (read-only)
         self.packed_provider = packed_provider
         self.pipeline = bool(pipeline)
+        self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
         self._slots: list[PackedWindow | None] = [None, None]
 
     def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:

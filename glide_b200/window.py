@@ -1,10 +1,11 @@
 """Device-side met windows: raw snapshot fields on the GPU and their packed bricks.
 
-``DeviceMet`` holds the raw float32 fields of the met snapshots on the device
-(the reference copies the window to the device once per window,
+``WindowFields`` holds the raw float32 fields of a window's two snapshots on the
+device (the reference copies the window to the device once per window,
 ``HannaScheme._cached_raw_device_met``, src/lpdm/turbulence/hanna.py:747-796);
 ``PackedWindow`` owns the three bricks the step kernel reads and fills them
-with ``glide_window_pack``.
+with ``glide_window_pack``; ``HostMetStreamer`` serves windows from host memory
+with prefetch.
 """
 
 from __future__ import annotations

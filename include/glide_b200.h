@@ -136,6 +136,9 @@ typedef struct glide_step_args {
     int32_t* escaped_per_step;               /* [n_steps] counters (added to), may be NULL */
     int32_t* active_per_step;                /* [n_steps] counters (added to), may be NULL */
     uint32_t* status;                        /* device status word (GLIDE_STATUS_*), may be NULL */
+    /* launch shape of the step kernel, 0 .. glide_step_launch_variants()-1 (block size
+     * and resident blocks per SM; 0 = 128 threads x 6 blocks). Results do not depend on it. */
+    int32_t launch_variant;
 } glide_step_args;
 
 /* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */
@@ -187,6 +190,11 @@ glide_status glide_window_pack(const glide_window_desc* desc, void* stream);
  * (FootprintGridder.accumulate, src/lpdm/footprint_gridder.py:117-197) and
  * escape kill (src/lpdm/main.py:1459-1477, 690-711). */
 glide_status glide_step(const glide_step_args* args, void* stream);
+
+/* Number of launch variants of the step kernel and, for variant v, its block size
+ * and the resident blocks per SM it is compiled for (autotuning). */
+glide_status glide_step_launch_variants(int32_t* count);
+glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t* min_blocks_per_sm);
 
 /* --- footprint accumulation alone -----------------------------------------------
  * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the

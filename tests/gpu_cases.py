@@ -19,7 +19,7 @@ def grid_of(run: GoldenRun) -> GridInfo:
 
 
 def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool = True, met_dtype: str = "f32",
-               seed: int = 1234, hanna_kw: dict | None = None) -> BatchRunner:
+               seed: int = 1234, hanna_kw: dict | None = None, launch_variant: int = 0) -> BatchRunner:
     z = run.z
     m = run.met
     grid = grid_of(run).to_device(device)
@@ -48,7 +48,7 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
 
     nxy = z["grid_nxy"]
     n_rel = int(z["release_idx"].max()) + 1
-    return BatchRunner(
+    runner = BatchRunner(
         grid=grid, window_provider=window_provider,
         hanna=HannaConfig(meander_enabled=bool(z["meander"]), max_substeps=ms, **(hanna_kw or {})),
         footprint=FootprintSpec(tuple(z["grid_lon"]), tuple(z["grid_lat"]), int(nxy[0]), int(nxy[1]),
@@ -59,6 +59,8 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
         noise_provider=noise_provider if injected else None,
         conv_uniform_provider=conv_provider if injected else None,
     )
+    runner.launch_variant = launch_variant
+    return runner
 
 
 def state_from(particles, rel_off, win_end, ridx, device, state: dict | None = None, alive=None) -> ParticleState:

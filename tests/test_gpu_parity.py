@@ -260,3 +260,25 @@ def test_ring_footprint_matches_dense(cuda_device):
     assert a.shape == b.shape and a.sum() > 0
     np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-7)
     assert r.footprint.device_shape[1] == 2
+
+
+def test_launch_variants_give_the_same_results(cuda_device):
+    """Every launch shape of the step kernel computes the same particles (the footprint
+    may differ in atomic summation order only); the autotuner picks one of them."""
+    from glide_b200.autotune import launch_variants, tune
+
+    run = load_run("run_small")
+    z = run.z
+    base = as_numpy(run_gpu(run, cuda_device))
+    for v, _, _ in launch_variants()[1:]:
+        got = as_numpy(run_gpu(run, cuda_device, launch_variant=v))
+        np.testing.assert_array_equal(got[0], base[0])
+        np.testing.assert_array_equal(got[2], base[2])
+        np.testing.assert_allclose(got[3], base[3], rtol=1e-5, atol=1e-9)
+    r = runner_for(run, cuda_device)
+    st = state_from(z["particles0"], z["rel_off"], z["win_end_off"], z["release_idx"], cuda_device)
+    res = tune(r, st, batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
+               cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]),
+               dt_seconds=float(z["dt_s"]), use_cache=False)
+    assert res["variant"] in [v for v, _, _ in launch_variants()]
+    assert r.launch_variant == res["variant"] and len(res["times_ms"]) == len(launch_variants())
