@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use launch variant 0 instead of tuning")
+    ap.add_argument("--no-reorder", action="store_true", help="step particles in index order (no work-class sort)")
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
@@ -710,6 +711,7 @@ def main() -> None:
                         domain=cfg["domain"], emanuel=cfg["emanuel"], met_dtype=args.met, device=dev,
                         seed=1234 + rank)
         r.launch_variant = tuned["variant"]
+        r.reorder = not args.no_reorder
         return r
 
     def fresh_state():
@@ -801,13 +803,14 @@ def main() -> None:
                        "max_substeps": 6, "step": "one met window (pack + convection + fused steps)",
                        "l2": "flushed (256 MB write) before every timed step; met bricks 440 MB > L2",
                        "parallelism": f"replicas x{world}", "launch_variant": tuned["variant"],
+                       "particle_order": "identity" if args.no_reorder else "work class, rebuilt per window",
                        "autotune_ms_per_window": {str(k): round(v, 3) for k, v in tuned["times_ms"].items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "kernel": "step_kernel", "bytes_per_particle_step": B_ALG[args.met],
                          "kernel_time_share": t_kernel / t_dev},
             "clocks": clk,
-            "gpu_launches": n_kernel_launches + 6 * args.steps,
+            "gpu_launches": n_kernel_launches + (6 if args.no_reorder else 9) * args.steps,
             "status": status,
         }
         if e2e is not None:

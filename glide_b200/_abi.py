@@ -16,7 +16,8 @@ LIB_PATH = Path(os.environ.get("GLIDE_B200_LIBRARY") or Path(__file__).resolve()
 
 GLIDE_OK = 0
 GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
-GLIDE_STATUS_NONFINITE_STATE = 1
+GLIDE_STATUS_NONFINITE_STATE, GLIDE_STATUS_BAD_ORDER = 1, 2
+GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 15, 16
 
 vp = C.c_void_p
 
@@ -58,7 +59,8 @@ class StepArgs(C.Structure):
                 ("noise_substep", vp), ("noise_meander", vp), ("seed", C.c_uint64), ("footprint", vp),
                 ("fp", FootprintGrid), ("dom_lon_min", C.c_double), ("dom_lon_max", C.c_double),
                 ("dom_lat_min", C.c_double), ("dom_lat_max", C.c_double), ("dom_alt_max", C.c_double),
-                ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32)]
+                ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32),
+                ("order", vp), ("work_key", vp)]
 
 
 class ConvectArgs(C.Structure):
@@ -83,6 +85,8 @@ SIGNATURES = {
     "glide_step": (C.c_int32, [C.POINTER(StepArgs), vp]),
     "glide_step_launch_variants": (C.c_int32, [C.POINTER(C.c_int32)]),
     "glide_step_launch_variant_info": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "glide_reorder_scratch_bytes": (C.c_int32, [C.c_int64, C.POINTER(C.c_size_t)]),
+    "glide_reorder_by_key": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_size_t, vp]),
     "glide_footprint_accumulate": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_float,
                                                C.POINTER(FootprintGrid), vp, vp]),
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),

@@ -54,6 +54,7 @@ struct StepDev {
     float dom_lon0, dom_lon1, dom_lat0, dom_lat1, dom_alt;
     int32_t* esc; int32_t* act;
     uint32_t* status;
+    const int32_t* order; uint8_t* work_key;
 };
 
 // ---------------------------------------------------------------------------
@@ -252,8 +253,15 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 template <typename T, int THREADS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev p) {
     extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool have = i < p.n;
+    const int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool have = th < p.n;
+    bool bad_order = false;
+    int64_t i = th;  // the particle this thread steps
+    if (have && p.order) {
+        const int64_t o = p.order[th];
+        if (o >= 0 && o < p.n) i = o;
+        else { have = false; bad_order = true; }
+    }
     const int lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < 2 * p.n_steps; k += blockDim.x) s_counts[k] = 0;
     __syncthreads();
@@ -284,12 +292,15 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
     // atomic) only when the cell (or time bin) changes, and at the end of the launch
     int64_t fp_cell = -1;
     float fp_acc = 0.0f;
+    int last_k = 1;         // substeps of the last physics step (work key)
+    bool last_active = false;
 
     for (int j = 0; j < p.n_steps; ++j) {
         const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
         bool active;
         if (p.active_mask) active = have && p.active_mask[i] != 0;
         else active = have && alive && (rel >= sc.cursor_off) && ((rel - L_sim) <= sc.cursor_off);
+        last_active = active;
 
         if (j >= p.phys_begin && active) {
             const float delta = sc.delta, alpha = sc.alpha;
@@ -410,6 +421,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
             if (!(kq == kq)) k = 1;  // NaN
             const float sub_dt = delta / (float)k;
+            last_k = k;
 
             // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
             const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
@@ -532,7 +544,17 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
         if (p.meander) { p.um[i] = um; p.vm[i] = vm; }
         if (p.alive) p.alive[i] = alive ? 1 : 0;
         if (nonfinite && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_NONFINITE_STATE);
+        if (p.work_key) {
+            int key = GLIDE_WORK_DONE;
+            if (alive) {
+                const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
+                if (!p.active_mask && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
+                else if (last_active) key = min(max(last_k, 1), GLIDE_WORK_PENDING - 1);
+            }
+            p.work_key[i] = (uint8_t)key;
+        }
     }
+    if (bad_order && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_BAD_ORDER);
     __syncthreads();
     for (int k = threadIdx.x; k < p.n_steps; k += blockDim.x) {
         if (p.esc && s_counts[k]) atomicAdd(p.esc + k, s_counts[k]);
@@ -626,6 +648,7 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.dom_alt = (float)a->dom_alt_max;
     d.esc = a->escaped_per_step; d.act = a->active_per_step;
     d.status = a->status;
+    d.order = a->order; d.work_key = a->work_key;
     cudaStream_t s = (cudaStream_t)stream;
     switch (a->met_dtype) {
         case GLIDE_MET_F32: return launch_step<float>(d, s, a->launch_variant);

@@ -249,6 +249,16 @@ class BatchRun:
             _abi.check(_abi.lib.glide_convect_scratch_bytes(runner.grid.shape[0], C.byref(nb)),
                        "glide_convect_scratch_bytes")
             self.conv_scratch = [torch.zeros(nb.value // 8, dtype=torch.float64, device=dev) for _ in range(2)]
+        # particle ordering by work class (glide_reorder_by_key): each window's launches step
+        # the particles in the order built from the work keys of the previous window
+        self.order = self.work_key = self.reorder_scratch = None
+        self.keys_valid = False
+        if runner.reorder and state.n > 0:
+            nb = C.c_size_t()
+            _abi.check(_abi.lib.glide_reorder_scratch_bytes(state.n, C.byref(nb)), "glide_reorder_scratch_bytes")
+            self.order = torch.empty(state.n, dtype=torch.int32, device=dev)
+            self.work_key = torch.zeros(state.n, dtype=torch.uint8, device=dev)
+            self.reorder_scratch = torch.empty(nb.value, dtype=torch.uint8, device=dev)
 
     @property
     def done(self) -> bool:
@@ -294,6 +304,9 @@ class BatchRun:
         a.active_per_step = self.act.data_ptr() + 4 * j0
         a.status = self.status.data_ptr()
         a.launch_variant = r.launch_variant
+        if self.work_key is not None:
+            a.order = self.order.data_ptr() if self.keys_valid else None
+            a.work_key = self.work_key.data_ptr()
         return a
 
     def _prepare(self, k: int) -> None:
@@ -347,6 +360,10 @@ class BatchRun:
         sh = stream_handle(main)
         n = j1 - j0
         with torch.cuda.stream(main):
+            if self.keys_valid:
+                _abi.check(_abi.lib.glide_reorder_by_key(self.state.n, self.work_key.data_ptr(), self.order.data_ptr(),
+                                                         self.reorder_scratch.data_ptr(),
+                                                         self.reorder_scratch.numel(), sh), "glide_reorder_by_key")
             if r.emanuel is not None:
                 a = self._step_args(packed, j0, 1, 0, 1, noise)
                 _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
@@ -356,6 +373,7 @@ class BatchRun:
             else:
                 a = self._step_args(packed, j0, n, 0, 0, noise)
                 _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+            self.keys_valid = self.work_key is not None
             done = torch.cuda.Event()
             done.record(main)
             self.slot_free[k % 2 if self.pipelined else 0] = done
@@ -483,6 +501,7 @@ class BatchRunner:
         self.packed_provider = packed_provider
         self.pipeline = bool(pipeline)
         self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
+        self.reorder = True  # group particles by work class each window (results do not depend on it)
         self._slots: list[PackedWindow | None] = [None, None]
 
     def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:

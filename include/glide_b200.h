@@ -34,7 +34,11 @@ enum { GLIDE_MET_F32 = 0, GLIDE_MET_BF16 = 1, GLIDE_MET_F16 = 2 };
 /* bits of the device status word (glide_step_args.status) */
 enum {
     GLIDE_STATUS_NONFINITE_STATE = 1u << 0, /* a particle's state became NaN/inf */
+    GLIDE_STATUS_BAD_ORDER = 1u << 1,       /* glide_step_args.order held an index outside [0, n) */
 };
+
+/* work classes written to glide_step_args.work_key */
+enum { GLIDE_WORK_DONE = 0, GLIDE_WORK_PENDING = 15, GLIDE_WORK_CLASSES = 16 };
 
 /* Met grid geometry: GridInterpolationBounds (src/lpdm/gpu_engine.py:100-121). */
 typedef struct glide_grid {
@@ -139,6 +143,16 @@ typedef struct glide_step_args {
     /* launch shape of the step kernel, 0 .. glide_step_launch_variants()-1 (block size
      * and resident blocks per SM; 0 = 128 threads x 6 blocks). Results do not depend on it. */
     int32_t launch_variant;
+    /* optional thread -> particle permutation, device [n] (NULL = identity): thread t steps
+     * particle order[t]. Results do not depend on it (state and noise are keyed by particle
+     * index); glide_reorder_by_key builds one that puts particles of equal work in the same
+     * warps. It must be a permutation of 0..n-1: an entry outside [0, n) is skipped and sets
+     * GLIDE_STATUS_BAD_ORDER; a repeated entry is not detected. */
+    const int32_t* order;
+    /* optional output, device [n] indexed by particle: the work class of the launch's last
+     * step, GLIDE_WORK_DONE (0, escaped or past the simulation length), 1 .. 14 (substeps
+     * taken, capped) or GLIDE_WORK_PENDING (15, alive but not yet released). */
+    uint8_t* work_key;
 } glide_step_args;
 
 /* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */
@@ -195,6 +209,18 @@ glide_status glide_step(const glide_step_args* args, void* stream);
  * and the resident blocks per SM it is compiled for (autotuning). */
 glide_status glide_step_launch_variants(int32_t* count);
 glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t* min_blocks_per_sm);
+
+/* --- particle ordering ---------------------------------------------------------
+ * No counterpart in the reference (its static path runs every particle through the
+ * same tensor ops). Builds order[0 .. n) for glide_step_args.order from a work_key
+ * written by the previous launch: descending work class (GLIDE_WORK_PENDING first,
+ * then 14 .. 1 substeps, GLIDE_WORK_DONE last), stable within a class, so that the
+ * lanes of a warp run the same number of substeps and the longest warps start first.
+ * Keys above 15 count as 15. Three launches on `stream`, no synchronisation; scratch
+ * is device memory of glide_reorder_scratch_bytes(n) bytes. n <= INT32_MAX. */
+glide_status glide_reorder_scratch_bytes(int64_t n, size_t* bytes);
+glide_status glide_reorder_by_key(int64_t n, const uint8_t* work_key, int32_t* order, void* scratch,
+                                  size_t scratch_bytes, void* stream);
 
 /* --- footprint accumulation alone -----------------------------------------------
  * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the

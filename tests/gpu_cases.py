@@ -19,7 +19,8 @@ def grid_of(run: GoldenRun) -> GridInfo:
 
 
 def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool = True, met_dtype: str = "f32",
-               seed: int = 1234, hanna_kw: dict | None = None, launch_variant: int = 0) -> BatchRunner:
+               seed: int = 1234, hanna_kw: dict | None = None, launch_variant: int = 0,
+               reorder: bool = True) -> BatchRunner:
     z = run.z
     m = run.met
     grid = grid_of(run).to_device(device)
@@ -60,6 +61,7 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
         conv_uniform_provider=conv_provider if injected else None,
     )
     runner.launch_variant = launch_variant
+    runner.reorder = reorder
     return runner
 
 
