@@ -168,35 +168,28 @@ __device__ __forceinline__ Sig6 bl_profile(float z, const Surface& s, int sl_ove
 // met sampling
 // ---------------------------------------------------------------------------
 
-// wind at (lon, lat, z): the RK2 wind function (hanna.py:866-889) returning
-// (dlon/dt, dlat/dt, w)
+// trilinear sample of the six leading channels of an 8-channel brick at
+// (lon, lat, z) (torch grid_sample, align_corners=True, zero padding; the
+// normalisation of gpu_engine.py:210-299); also returns the grid x / y indices
 template <typename T>
-__device__ __forceinline__ float3 wind_at(const StepDev& p, float lon, float lat, float z, float alpha) {
-    const GridDev& g = p.g;
-    const float xn = norm_h(lon, g.lon0, g.lon_span);
-    const float yn = norm_h(lat, g.lat0, g.lat_span);
-    const float zn = norm_z(z, g);
+__device__ __forceinline__ void sample6(const T* brick, const GridDev& g, float lon, float lat, float z, float acc[6],
+                                        float& ix, float& iy) {
+    ix = unnorm(norm_h(lon, g.lon0, g.lon_span), (float)(g.nx - 1));
+    iy = unnorm(norm_h(lat, g.lat0, g.lat_span), (float)(g.ny - 1));
     Tri t;
-    tri_weights(unnorm(xn, (float)(g.nx - 1)), unnorm(yn, (float)(g.ny - 1)), unnorm(zn, g.zmax_idx), g.nx, g.ny,
-                g.nz, t);
-    const T* wb = static_cast<const T*>(p.wind);
-    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    tri_weights(ix, iy, unnorm(norm_z(z, g), g.zmax_idx), g.nx, g.ny, g.nz, t);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = 0.f;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const int zz = (c & 4) ? t.z1 : t.z0;
         const int yy = (c & 2) ? t.y1 : t.y0;
         const int xx = (c & 1) ? t.x1 : t.x0;
         float v[8];
-        load8(wb + cell_index(zz, yy, xx, g.ny, g.nx) * 8, v);
+        load8(brick + cell_index(zz, yy, xx, g.ny, g.nx) * 8, v);
 #pragma unroll
         for (int k = 0; k < 6; ++k) acc[k] = acc[k] + v[k] * t.w[c];
     }
-    const float om = 1.0f - alpha;
-    const float u = acc[0] * om + acc[3] * alpha;
-    const float vv = acc[1] * om + acc[4] * alpha;
-    const float w = acc[2] * om + acc[5] * alpha;
-    const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
-    return make_float3(u / m_lon, vv / M_PER_DEG_LAT, w);
 }
 
 template <typename T>
@@ -249,8 +242,15 @@ __device__ __forceinline__ float noise_or_philox(const StepDev& p, const float* 
 struct LaunchShape { int threads, min_blocks; };
 constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+// variant kNumShapes: the general kernel at shape 0 whatever the arguments
+constexpr int kNumVariants = kNumShapes + 1;
 
-template <typename T, int THREADS, int MIN_BLOCKS>
+// GENERAL = false compiles out the paths the production configuration never
+// takes (surface-layer override, injected noise, caller-supplied active mask):
+// the kernel is smaller, which matters because it is bound by instruction
+// issue and instruction-cache misses. Arguments that need one of those paths
+// run the GENERAL = true instantiation; both compute identical results.
+template <typename T, int THREADS, int MIN_BLOCKS, bool GENERAL>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev p) {
     extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
     const int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -298,28 +298,55 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
     for (int j = 0; j < p.n_steps; ++j) {
         const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
         bool active;
-        if (p.active_mask) active = have && p.active_mask[i] != 0;
+        if (GENERAL && p.active_mask) active = have && p.active_mask[i] != 0;
         else active = have && alive && (rel >= sc.cursor_off) && ((rel - L_sim) <= sc.cursor_off);
         last_active = active;
 
         if (j >= p.phys_begin && active) {
             const float delta = sc.delta, alpha = sc.alpha;
-            // --- RK2 midpoint advection, backward (hanna.py:855-896)
+            // --- RK2 midpoint advection, backward (hanna.py:855-896), then the support
+            // brick at z_eval. One sampling loop serves all three trilinear samples (one
+            // copy of the level search and gather in the code): stage 0 the wind at the
+            // start point, stage 1 at the midpoint (hanna.py:866-889, two snapshots lerped
+            // by alpha), stage 2 the support brick (FT sigma_w / T_Lw, rho, drho/dz,
+            // meander sigmas) at the advected position and z_eval = max(z, z_ubl).
+            const GridDev& g = p.g;
+            const float z_ubl = p.z_ubl;
+            float acc[6];
+            float ix, iy;
             {
                 const float hd = 0.5f * delta;
                 float qx = lon, qy = lat, qz = z;
-                float3 v;
 #pragma unroll 1
-                for (int stage = 0; stage < 2; ++stage) {
-                    v = wind_at<T>(p, qx, qy, qz, alpha);
-                    qx = lon - hd * v.x;
-                    qy = lat - hd * v.y;
-                    qz = z - hd * v.z;
+                for (int stage = 0; stage < 3; ++stage) {
+                    sample6<T>(static_cast<const T*>(stage < 2 ? p.wind : p.support), g, qx, qy, qz, acc, ix, iy);
+                    if (stage < 2) {
+                        const float om = 1.0f - alpha;
+                        const float u = acc[0] * om + acc[3] * alpha;
+                        const float vv = acc[1] * om + acc[4] * alpha;
+                        const float w = acc[2] * om + acc[5] * alpha;
+                        const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(qy * DEG2RAD)), 0.05f);
+                        const float vx = u / m_lon, vy = vv / M_PER_DEG_LAT;
+                        if (stage == 0) {
+                            qx = lon - hd * vx;
+                            qy = lat - hd * vy;
+                            qz = z - hd * w;
+                        } else {
+                            lon = lon - delta * vx;
+                            lat = lat - delta * vy;
+                            z = z - delta * w;
+                            qx = lon;
+                            qy = lat;
+                            qz = fmaxf(z, z_ubl);
+                        }
+                    }
                 }
-                lon = lon - delta * v.x;
-                lat = lat - delta * v.y;
-                z = z - delta * v.z;
             }
+            const float z_eval = fmaxf(z, z_ubl);
+            const float ft_sw = acc[0], ft_tl = acc[1];
+            const float rho_p = acc[2];
+            const float drho_p = acc[3] * Scales<T>::drho;
+            const float m_su = acc[4], m_sv = acc[5];
 
             // --- surface fields and stability (hanna.py:950-966, 142-189)
             float sf[5];
@@ -341,36 +368,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                 S.f_abs = fmaxf(fabsf(f_cor), 1e-5f);
             }
 
-            // --- support brick at z_eval: FT sigma_w / T_Lw, rho, drho/dz, meander sigmas
-            const float z_ubl = p.z_ubl;
-            const float z_eval = fmaxf(z, z_ubl);
-            const GridDev& g = p.g;
-            const float ix = unnorm(norm_h(lon, g.lon0, g.lon_span), (float)(g.nx - 1));
-            const float iy = unnorm(norm_h(lat, g.lat0, g.lat_span), (float)(g.ny - 1));
-            const float iz_e = unnorm(norm_z(z_eval, g), g.zmax_idx);
-            Tri t;
-            tri_weights(ix, iy, iz_e, g.nx, g.ny, g.nz, t);
-            const T* sup = static_cast<const T*>(p.support);
-            float ftsw_c[8];
-            float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int zz = (c & 4) ? t.z1 : t.z0;
-                const int yy = (c & 2) ? t.y1 : t.y0;
-                const int xx = (c & 1) ? t.x1 : t.x0;
-                float v[8];
-                load8(sup + cell_index(zz, yy, xx, g.ny, g.nx) * 8, v);
-                ftsw_c[c] = v[0];
-#pragma unroll
-                for (int k = 0; k < 6; ++k) acc[k] = acc[k] + v[k] * t.w[c];
-            }
-            const float ft_sw = acc[0], ft_tl = acc[1];
-            const float rho_p = acc[2];
-            const float drho_p = acc[3] * Scales<T>::drho;
-            const float m_su = acc[4], m_sv = acc[5];
-
             // --- column turbulence at z_eval (hanna.py:976-982)
-            Sig6 col = bl_profile(z_eval, S, p.sl_override, p.floors);
+            Sig6 col = bl_profile(z_eval, S, GENERAL ? p.sl_override : 0, p.floors);
             if (z_eval > S.blh) {
                 col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
                 col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
@@ -385,23 +384,19 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
 #pragma unroll 1
             for (int q = 0; q < 2; ++q) {
                 const float zq = q == 0 ? z_hi : z_lo;
-                float s = bl_sigma_w(zq, S, p.sl_override);
-                if (zq > S.blh) {
+                float s = bl_sigma_w(zq, S, GENERAL ? p.sl_override : 0);
+                if (zq > S.blh) {  // free-troposphere sigma_w from the support brick's channel 0
                     const float izq = unnorm(norm_z(zq, g), g.zmax_idx);
                     Tri tq;
                     tri_weights(ix, iy, izq, g.nx, g.ny, g.nz, tq);
+                    const T* sup = static_cast<const T*>(p.support);
                     float a = 0.f;
-                    if (tq.z0 == t.z0 && tq.z1 == t.z1) {
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) a = a + ftsw_c[c] * tq.w[c];
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            const int zz = (c & 4) ? tq.z1 : tq.z0;
-                            const int yy = (c & 2) ? tq.y1 : tq.y0;
-                            const int xx = (c & 1) ? tq.x1 : tq.x0;
-                            a = a + to_f(sup[cell_index(zz, yy, xx, g.ny, g.nx) * 8]) * tq.w[c];
-                        }
+                    for (int c = 0; c < 8; ++c) {
+                        const int zz = (c & 4) ? tq.z1 : tq.z0;
+                        const int yy = (c & 2) ? tq.y1 : tq.y0;
+                        const int xx = (c & 1) ? tq.x1 : tq.x0;
+                        a = a + to_f(sup[cell_index(zz, yy, xx, g.ny, g.nx) * 8]) * tq.w[c];
                     }
                     s = a;
                 }
@@ -434,7 +429,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
             for (int it = 0; it < k; ++it) {
                 float eu, ev, ew;
-                if (p.noise_sub) {
+                if (GENERAL && p.noise_sub) {
                     const float* b = p.noise_sub + ((int64_t)(j * ms + it) * 3) * nn + i;
                     eu = __ldg(b);
                     ev = __ldg(b + nn);
@@ -466,7 +461,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             // --- meander (hanna.py:1028-1054)
             if (p.meander) {
                 float e0, e1;
-                if (p.noise_mea) {
+                if (GENERAL && p.noise_mea) {
                     const float* b = p.noise_mea + ((int64_t)j * 2) * nn + i;
                     e0 = __ldg(b);
                     e1 = __ldg(b + nn);
@@ -548,7 +543,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             int key = GLIDE_WORK_DONE;
             if (alive) {
                 const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
-                if (!p.active_mask && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
+                if (!(GENERAL && p.active_mask) && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
                 else if (last_active) key = min(max(last_k, 1), GLIDE_WORK_PENDING - 1);
             }
             p.work_key[i] = (uint8_t)key;
@@ -562,11 +557,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
     }
 }
 
-template <typename T, int V>
+template <typename T, int V, bool GENERAL>
 static void launch_shape(const StepDev& d, cudaStream_t stream, size_t smem) {
     constexpr int threads = kShapes[V].threads;
     const int64_t blocks = (d.n + threads - 1) / threads;
-    step_kernel<T, threads, kShapes[V].min_blocks><<<(unsigned)blocks, threads, smem, stream>>>(d);
+    step_kernel<T, threads, kShapes[V].min_blocks, GENERAL><<<(unsigned)blocks, threads, smem, stream>>>(d);
 }
 
 template <typename T>
@@ -574,11 +569,12 @@ static glide_status launch_step(const StepDev& d, cudaStream_t stream, int varia
     const size_t smem = sizeof(int32_t) * 2 * (size_t)d.n_steps;
     if (smem > 48 * 1024) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large", d.n_steps);
     switch (variant) {
-        case 0: launch_shape<T, 0>(d, stream, smem); break;
-        case 1: launch_shape<T, 1>(d, stream, smem); break;
-        case 2: launch_shape<T, 2>(d, stream, smem); break;
-        case 3: launch_shape<T, 3>(d, stream, smem); break;
-        case 4: launch_shape<T, 4>(d, stream, smem); break;
+        case 0: launch_shape<T, 0, false>(d, stream, smem); break;
+        case 1: launch_shape<T, 1, false>(d, stream, smem); break;
+        case 2: launch_shape<T, 2, false>(d, stream, smem); break;
+        case 3: launch_shape<T, 3, false>(d, stream, smem); break;
+        case 4: launch_shape<T, 4, false>(d, stream, smem); break;
+        case kNumShapes: launch_shape<T, 0, true>(d, stream, smem); break;
         default: return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", variant);
     }
     return check_launch("glide_step");
@@ -606,7 +602,7 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (a->grid.nz < 2 || a->grid.ny < 2 || a->grid.nx < 2)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: grid must be at least 2x2x2");
     if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
-    if (a->launch_variant < 0 || a->launch_variant >= kNumShapes)
+    if (a->launch_variant < 0 || a->launch_variant >= kNumVariants)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", a->launch_variant);
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
     if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
@@ -650,24 +646,27 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.status = a->status;
     d.order = a->order; d.work_key = a->work_key;
     cudaStream_t s = (cudaStream_t)stream;
+    const bool general = d.sl_override || d.noise_sub || d.noise_mea || d.active_mask;
+    const int variant = general ? kNumShapes : a->launch_variant;
     switch (a->met_dtype) {
-        case GLIDE_MET_F32: return launch_step<float>(d, s, a->launch_variant);
-        case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s, a->launch_variant);
-        case GLIDE_MET_F16: return launch_step<__half>(d, s, a->launch_variant);
+        case GLIDE_MET_F32: return launch_step<float>(d, s, variant);
+        case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s, variant);
+        case GLIDE_MET_F16: return launch_step<__half>(d, s, variant);
         default: return set_error(GLIDE_ERR_UNSUPPORTED, "glide_step: unknown met_dtype %d", a->met_dtype);
     }
 }
 
 extern "C" glide_status glide_step_launch_variants(int32_t* count) {
     if (!count) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_launch_variants: count is NULL");
-    *count = kNumShapes;
+    *count = kNumVariants;
     return GLIDE_OK;
 }
 
 extern "C" glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t* min_blocks) {
-    if (v < 0 || v >= kNumShapes)
+    if (v < 0 || v >= kNumVariants)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_launch_variant_info: variant %d out of range", v);
-    if (threads) *threads = kShapes[v].threads;
-    if (min_blocks) *min_blocks = kShapes[v].min_blocks;
+    const LaunchShape sh = kShapes[v < kNumShapes ? v : 0];
+    if (threads) *threads = sh.threads;
+    if (min_blocks) *min_blocks = sh.min_blocks;
     return GLIDE_OK;
 }

@@ -140,8 +140,10 @@ typedef struct glide_step_args {
     int32_t* escaped_per_step;               /* [n_steps] counters (added to), may be NULL */
     int32_t* active_per_step;                /* [n_steps] counters (added to), may be NULL */
     uint32_t* status;                        /* device status word (GLIDE_STATUS_*), may be NULL */
-    /* launch shape of the step kernel, 0 .. glide_step_launch_variants()-1 (block size
-     * and resident blocks per SM; 0 = 128 threads x 6 blocks). Results do not depend on it. */
+    /* launch variant of the step kernel, 0 .. glide_step_launch_variants()-1: block size and
+     * resident blocks per SM (0 = 128 threads x 6 blocks). The last variant is the general
+     * kernel at shape 0, which every launch that sets surface_layer_override, injected noise
+     * or active_mask runs whatever this field says. Results do not depend on it. */
     int32_t launch_variant;
     /* optional thread -> particle permutation, device [n] (NULL = identity): thread t steps
      * particle order[t]. Results do not depend on it (state and noise are keyed by particle
@@ -206,7 +208,8 @@ glide_status glide_window_pack(const glide_window_desc* desc, void* stream);
 glide_status glide_step(const glide_step_args* args, void* stream);
 
 /* Number of launch variants of the step kernel and, for variant v, its block size
- * and the resident blocks per SM it is compiled for (autotuning). */
+ * and the resident blocks per SM it is compiled for (autotuning; the last variant is
+ * the general kernel, see glide_step_args.launch_variant). */
 glide_status glide_step_launch_variants(int32_t* count);
 glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t* min_blocks_per_sm);
 

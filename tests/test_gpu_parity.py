@@ -263,22 +263,28 @@ def test_ring_footprint_matches_dense(cuda_device):
 
 
 def test_launch_variants_give_the_same_results(cuda_device):
-    """Every launch shape of the step kernel computes the same particles (the footprint
-    may differ in atomic summation order only); the autotuner picks one of them."""
+    """Every launch variant computes the same particles (the footprint may differ in
+    atomic summation order only): the fast kernels at every shape against the general
+    kernel (the last variant, which the injected-noise parity runs use), on generated
+    noise and on every met storage type; the autotuner picks one of them."""
     from glide_b200.autotune import launch_variants, tune
 
     run = load_run("run_small")
     z = run.z
-    base = as_numpy(run_gpu(run, cuda_device))
-    for v, _, _ in launch_variants()[1:]:
-        got = as_numpy(run_gpu(run, cuda_device, launch_variant=v))
-        np.testing.assert_array_equal(got[0], base[0])
-        np.testing.assert_array_equal(got[2], base[2])
-        np.testing.assert_allclose(got[3], base[3], rtol=1e-5, atol=1e-9)
-    r = runner_for(run, cuda_device)
+    variants = [v for v, _, _ in launch_variants()]
+    for met_dtype in ("f32", "bf16", "f16"):
+        base = as_numpy(run_gpu(run, cuda_device, injected=False, met_dtype=met_dtype, launch_variant=variants[-1]))
+        for v in variants[:-1]:
+            got = as_numpy(run_gpu(run, cuda_device, injected=False, met_dtype=met_dtype, launch_variant=v))
+            np.testing.assert_array_equal(got[0], base[0])
+            for k in base[1]:
+                np.testing.assert_array_equal(got[1][k], base[1][k])
+            np.testing.assert_array_equal(got[2], base[2])
+            np.testing.assert_allclose(got[3], base[3], rtol=1e-5, atol=1e-9)
+    r = runner_for(run, cuda_device, injected=False)
     st = state_from(z["particles0"], z["rel_off"], z["win_end_off"], z["release_idx"], cuda_device)
     res = tune(r, st, batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
                cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]),
                dt_seconds=float(z["dt_s"]), use_cache=False)
-    assert res["variant"] in [v for v, _, _ in launch_variants()]
-    assert r.launch_variant == res["variant"] and len(res["times_ms"]) == len(launch_variants())
+    assert res["variant"] in variants
+    assert r.launch_variant == res["variant"] and len(res["times_ms"]) == len(variants)
