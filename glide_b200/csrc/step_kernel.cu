@@ -67,14 +67,31 @@ struct Surface {
 
 struct Sig6 { float su, sv, sw, tlu, tlv, tlw; };
 
-__device__ __forceinline__ Sig6 in_bl(float z, const Surface& s) {
+// sigma_w of the three regimes (no surface-layer override)
+__device__ __forceinline__ float sigma_w_bl(float z, const Surface& s) {
+    const float blh = s.blh, us = s.ustar;
+    if (s.hL > 1.0f) {
+        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
+        return (1.3f * us) * fmaxf(1.0f - zoh, 0.0f);
+    }
+    if (s.hL < -1.0f) {
+        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
+        const float sw2 = (((1.2f * (s.w_star * s.w_star)) * fmaxf(1.0f - 0.9f * zoh, 0.0f))
+                           * powf(zoh, 2.0f / 3.0f)) + ((1.8f - 1.4f * zoh) * (us * us));
+        return sqrtf(fmaxf(sw2, SIGMA_MIN * SIGMA_MIN));
+    }
+    return (1.3f * us) * expf(((-2.0f * s.f_abs) * z) / us);
+}
+
+// the other five outputs of the regimes given sw = sigma_w_bl(z, s)
+__device__ __forceinline__ Sig6 in_bl(float z, const Surface& s, float sw) {
     Sig6 o;
     const float blh = s.blh, us = s.ustar;
+    o.sw = sw;
     if (s.hL > 1.0f) {  // stable (hanna.py:192-222)
         const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
         const float om = fmaxf(1.0f - zoh, 0.0f);
         o.su = (2.0f * us) * om;
-        o.sw = (1.3f * us) * om;
         o.sv = o.sw;
         const float zf = fmaxf(zoh, 1e-6f);
         const float sq = sqrtf(zf);
@@ -86,9 +103,6 @@ __device__ __forceinline__ Sig6 in_bl(float z, const Surface& s) {
         const float hl = fminf(fmaxf(s.hL, -1000.0f), 0.0f);
         o.su = powf(fmaxf(12.0f - 0.5f * hl, 1e-3f), 1.0f / 3.0f) * us;
         o.sv = o.su;
-        const float sw2 = (((1.2f * (s.w_star * s.w_star)) * fmaxf(1.0f - 0.9f * zoh, 0.0f))
-                           * powf(zoh, 2.0f / 3.0f)) + ((1.8f - 1.4f * zoh) * (us * us));
-        o.sw = sqrtf(fmaxf(sw2, SIGMA_MIN * SIGMA_MIN));
         o.tlu = (0.15f * blh) / fmaxf(o.su, SIGMA_MIN);
         o.tlv = o.tlu;
         const float azl = fmaxf(zoh * (-hl), 0.0f);
@@ -103,7 +117,6 @@ __device__ __forceinline__ Sig6 in_bl(float z, const Surface& s) {
     } else {  // neutral (hanna.py:225-252)
         const float fa = s.f_abs;
         o.su = (2.0f * us) * expf(((-3.0f * fa) * z) / us);
-        o.sw = (1.3f * us) * expf(((-2.0f * fa) * z) / us);
         o.sv = o.sw;
         const float den = 1.0f + (((15.0f * fa) * z) / us);
         o.tlw = ((0.5f * z) / fmaxf(o.sw, SIGMA_MIN)) / fmaxf(den, 1.0f);
@@ -124,29 +137,19 @@ __device__ __forceinline__ float sl_sigma_w(float z, float us, float L) {
 // sigma_w alone of bl_profile (the z_eval +- 1 m probes of the well-mixed drift
 // need nothing else; floors only touch the timescales)
 __device__ __forceinline__ float bl_sigma_w(float z, const Surface& s, int sl_override) {
-    const float blh = s.blh, us = s.ustar;
-    if (sl_override && z < 0.1f * blh) return sl_sigma_w(z, us, s.L);
-    if (s.hL > 1.0f) {
-        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
-        return (1.3f * us) * fmaxf(1.0f - zoh, 0.0f);
-    }
-    if (s.hL < -1.0f) {
-        const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
-        const float sw2 = (((1.2f * (s.w_star * s.w_star)) * fmaxf(1.0f - 0.9f * zoh, 0.0f))
-                           * powf(zoh, 2.0f / 3.0f)) + ((1.8f - 1.4f * zoh) * (us * us));
-        return sqrtf(fmaxf(sw2, SIGMA_MIN * SIGMA_MIN));
-    }
-    return (1.3f * us) * expf(((-2.0f * s.f_abs) * z) / us);
+    if (sl_override && z < 0.1f * s.blh) return sl_sigma_w(z, s.ustar, s.L);
+    return sigma_w_bl(z, s);
 }
 
 // BL profile + optional surface-layer override + FLEXPART floors, before the
 // free-troposphere override (hanna.py:1529-1565)
-__device__ __forceinline__ Sig6 bl_profile(float z, const Surface& s, int sl_override, int floors) {
-    Sig6 o = in_bl(z, s);
+__device__ __forceinline__ Sig6 bl_profile(float z, const Surface& s, int sl_override, int floors, float sw_z) {
+    Sig6 o = in_bl(z, s, sw_z);
     if (sl_override) {
         const float z_sl = 0.1f * s.blh;
         if (z < z_sl) {
-            const Sig6 c = in_bl(fmaxf(z, z_sl), s);
+            const float zc = fmaxf(z, z_sl);
+            const Sig6 c = in_bl(zc, s, sigma_w_bl(zc, s));
             o.su = c.su;
             o.sv = c.sv;
             o.sw = sl_sigma_w(z, s.ustar, s.L);
@@ -368,24 +371,19 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                 S.f_abs = fmaxf(fabsf(f_cor), 1e-5f);
             }
 
-            // --- column turbulence at z_eval (hanna.py:976-982)
-            Sig6 col = bl_profile(z_eval, S, GENERAL ? p.sl_override : 0, p.floors);
-            if (z_eval > S.blh) {
-                col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
-                col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
-            }
-            const float su = fmaxf(col.su, SIGMA_MIN), sv = fmaxf(col.sv, SIGMA_MIN), sw = fmaxf(col.sw, SIGMA_MIN);
-            const float tlu = fmaxf(col.tlu, T_L_MIN), tlv = fmaxf(col.tlv, T_L_MIN), tlw = fmaxf(col.tlw, T_L_MIN);
-
-            // --- sigma_w at z_eval +- 1 m for the well-mixed drift (hanna.py:984-991)
-            float sw_pm[2];
+            // --- sigma_w: the BL profile's at z_eval (column turbulence) and the closure's
+            // at z_eval +- 1 m for the well-mixed drift (hanna.py:984-991; above the BL the
+            // free-troposphere value from the support brick's channel 0). One rolled loop
+            // keeps one copy of the regime code.
+            const int sl = GENERAL ? p.sl_override : 0;
             const float z_hi = z_eval + 1.0f;
             const float z_lo = fmaxf(z_eval - 1.0f, z_ubl);
+            float sw_col = 0.f, sw_hi = 0.f, sw_lo = 0.f;
 #pragma unroll 1
-            for (int q = 0; q < 2; ++q) {
-                const float zq = q == 0 ? z_hi : z_lo;
-                float s = bl_sigma_w(zq, S, GENERAL ? p.sl_override : 0);
-                if (zq > S.blh) {  // free-troposphere sigma_w from the support brick's channel 0
+            for (int q = 0; q < 3; ++q) {
+                const float zq = q == 0 ? z_eval : (q == 1 ? z_hi : z_lo);
+                float s = bl_sigma_w(zq, S, q == 0 ? 0 : sl);
+                if (q > 0 && zq > S.blh) {
                     const float izq = unnorm(norm_z(zq, g), g.zmax_idx);
                     Tri tq;
                     tri_weights(ix, iy, izq, g.nx, g.ny, g.nz, tq);
@@ -400,9 +398,21 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                     }
                     s = a;
                 }
-                sw_pm[q] = fmaxf(s, SIGMA_MIN);
+                if (q == 0) sw_col = s;
+                else if (q == 1) sw_hi = fmaxf(s, SIGMA_MIN);
+                else sw_lo = fmaxf(s, SIGMA_MIN);
             }
-            const float dsig2 = (sw_pm[0] * sw_pm[0] - sw_pm[1] * sw_pm[1]) / fmaxf(z_hi - z_lo, 1.0f);
+
+            // --- column turbulence at z_eval (hanna.py:976-982)
+            Sig6 col = bl_profile(z_eval, S, sl, p.floors, sw_col);
+            if (z_eval > S.blh) {
+                col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
+                col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
+            }
+            const float su = fmaxf(col.su, SIGMA_MIN), sv = fmaxf(col.sv, SIGMA_MIN), sw = fmaxf(col.sw, SIGMA_MIN);
+            const float tlu = fmaxf(col.tlu, T_L_MIN), tlv = fmaxf(col.tlv, T_L_MIN), tlw = fmaxf(col.tlw, T_L_MIN);
+
+            const float dsig2 = (sw_hi * sw_hi - sw_lo * sw_lo) / fmaxf(z_hi - z_lo, 1.0f);
             const float sw_sq = fmaxf(sw * sw, SIGMA_MIN * SIGMA_MIN);
 
             // --- density drift (hanna.py:993-1006)
@@ -493,6 +503,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                 const float xf = floorf(((lon - p.fp_lon0) / p.fp_lon_span) * (float)p.fp_X);
                 const float yf = floorf(((lat - p.fp_lat0) / p.fp_lat_span) * (float)p.fp_Y);
                 int zb = 0;
+#pragma unroll 1
                 for (int e = 0; e <= p.fp_Z; ++e) zb += (__ldg(p.fp_edges + e) < z) ? 1 : 0;
                 zb -= 1;
                 valid = (rid >= 0) && (rid < p.fp_R) && (xf >= 0.0f) && (xf < (float)p.fp_X) && (yf >= 0.0f) &&
