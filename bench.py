@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use launch variant 0 instead of tuning")
     ap.add_argument("--no-reorder", action="store_true", help="step particles in index order (no work-class sort)")
+    ap.add_argument("--no-pipeline", action="store_true", help="prepare each window inline (no side stream)")
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
@@ -709,7 +710,7 @@ def main() -> None:
     def make_runner(provider):
         r = BatchRunner(grid=grid, window_provider=provider, hanna=cfg["hanna"], footprint=cfg["footprint"],
                         domain=cfg["domain"], emanuel=cfg["emanuel"], met_dtype=args.met, device=dev,
-                        seed=1234 + rank)
+                        seed=1234 + rank, pipeline=not args.no_pipeline)
         r.launch_variant = tuned["variant"]
         r.reorder = not args.no_reorder
         return r
@@ -733,12 +734,13 @@ def main() -> None:
     kernel_events: list = []
     real_step = abi.lib.glide_step
 
-    def timed_step(a, s):
+    def timed_step(a, s):  # events on the stream the kernel is launched on
+        ls = torch.cuda.ExternalStream(s, device=dev) if s else stream
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(ls)
         rc = real_step(a, s)
-        e1.record(stream)
+        e1.record(ls)
         if record_kernels:
             kernel_events.append((e0, e1))
         return rc

@@ -343,7 +343,8 @@ class BatchRun:
         j0, j1 = self.windows[k]
         self.next_window += 1
         first = self.steps[j0]
-        main = stream if stream is not None else torch.cuda.current_stream(r.device)
+        caller = stream if stream is not None else torch.cuda.current_stream(r.device)
+        main = stream if stream is not None else r.step_stream
         if k not in self.prepared:
             self._prepare(k)
         wf, packed, scratch, ready = self.prepared.pop(k)
@@ -357,6 +358,8 @@ class BatchRun:
             if r.hanna.meander_enabled and (mea is None or tuple(mea.shape) != (j1 - j0, 2, self.state.n)
                                             or mea.dtype != torch.float32 or not mea.is_contiguous()):
                 raise ValueError("injected meander noise must be contiguous float32 (steps, 2, n)")
+        if main is not caller:  # the caller's work so far (state, noise) comes first
+            main.wait_stream(caller)
         sh = stream_handle(main)
         n = j1 - j0
         with torch.cuda.stream(main):
@@ -384,6 +387,8 @@ class BatchRun:
                 prov.window_done(first.hour)
                 if not self.done:
                     prov.prefetch(self.steps[self.windows[self.next_window][0]].hour)
+        if main is not caller:  # later work on the caller's stream sees this window's results
+            caller.wait_stream(main)
         if self.pipelined and not self.done:
             self._prepare(self.next_window)  # overlaps this window's steps
         return True
@@ -502,7 +507,19 @@ class BatchRunner:
         self.pipeline = bool(pipeline)
         self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
         self.reorder = True  # group particles by work class each window (results do not depend on it)
+        self._step_stream = None
         self._slots: list[PackedWindow | None] = [None, None]
+
+    @property
+    def step_stream(self) -> torch.cuda.Stream:
+        """The stream a batch's launches run on when ``step_window`` is given none: a
+        high-priority stream, so that the block scheduler runs the step kernel's blocks
+        ahead of the next window's preparation (packing, column build) on the side stream,
+        which then fills the SMs the step kernel leaves idle."""
+        if self._step_stream is None:
+            lo, hi = torch.cuda.Stream.priority_range()
+            self._step_stream = torch.cuda.Stream(device=self.device, priority=hi)
+        return self._step_stream
 
     def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:
         """The packed bricks of ``wf`` (packed into brick slot ``slot`` unless a
