@@ -72,7 +72,13 @@ class ConvectArgs(C.Structure):
                 ("uniforms", vp), ("seed", C.c_uint64), ("scratch", vp), ("n_moved", vp)]
 
 
-STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs)
+class OuArgs(C.Structure):
+    _fields_ = [("n", C.c_int64), ("w", vp), ("t_l", vp), ("t_l_scalar", C.c_float), ("sigma2", vp),
+                ("sigma2_scalar", C.c_float), ("dt", vp), ("dt_scalar", C.c_float), ("drift", vp),
+                ("drift_scalar", C.c_float), ("noise", vp), ("seed", C.c_uint64), ("counter", C.c_uint32)]
+
+
+STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs)
 
 # every exported symbol with (restype, argtypes)
 SIGNATURES = {
@@ -87,6 +93,11 @@ SIGNATURES = {
     "glide_step_launch_variant_info": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "glide_reorder_scratch_bytes": (C.c_int32, [C.c_int64, C.POINTER(C.c_size_t)]),
     "glide_reorder_by_key": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_size_t, vp]),
+    "glide_ou_update": (C.c_int32, [C.POINTER(OuArgs), vp]),
+    "glide_displace_vertical": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, vp, C.c_float, C.c_int32, vp]),
+    "glide_displace_horizontal": (C.c_int32, [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_float, C.c_int32, vp]),
+    "glide_reflect_surface": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, C.c_float, vp]),
+    "glide_rk2_stage": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, C.c_int64, C.c_float, vp, C.c_int64, vp]),
     "glide_footprint_accumulate": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_float,
                                                C.POINTER(FootprintGrid), vp, vp]),
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),

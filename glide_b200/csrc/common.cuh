@@ -277,4 +277,38 @@ __device__ __forceinline__ float torch_lerp(float s, float e, float w) {
     return (fabsf(w) < 0.5f) ? __fmaf_rn(w, d, s) : __fmaf_rn(w - 1.0f, d, e);
 }
 
+// ---------------------------------------------------------------------------
+// Particle-update arithmetic shared by the fused step kernel and the engine
+// primitives (src/lpdm/gpu_engine.py:26-42, 345-507), in the reference's
+// operation order.
+// ---------------------------------------------------------------------------
+
+// exact Ornstein-Uhlenbeck step: decay a = exp(-dt / T_L), noise amplitude
+// sqrt(max(sigma^2 (1 - a^2), 0)), update a w + drift dt + amplitude eta
+__device__ __forceinline__ float ou_decay(float dt, float tl) { return expf(-dt / tl); }
+__device__ __forceinline__ float ou_amplitude(float sigma2, float a) { return sqrtf(fmaxf(sigma2 * (1.0f - a * a), 0.0f)); }
+__device__ __forceinline__ float ou_step(float prev, float a, float drift_dt, float amp, float eta) {
+    return (a * prev + drift_dt) + amp * eta;
+}
+
+// metres per degree of longitude at a latitude (cos clamped at 0.05)
+__device__ __forceinline__ float m_per_deg_lon(float lat) { return M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f); }
+
+// displacement by a velocity over dt in the given direction (-1 backward, +1 forward)
+__device__ __forceinline__ float displace_z(float z, float w, float dt, float dir) { return z + (dir * w) * dt; }
+__device__ __forceinline__ float displace_lon(float lon, float u, float dt, float dir, float m_lon) {
+    return lon + ((dir * u) * dt) / m_lon;
+}
+__device__ __forceinline__ float displace_lat(float lat, float v, float dt, float dir) {
+    return lat + ((dir * v) * dt) / M_PER_DEG_LAT;
+}
+
+// smooth-wall reflection at z_surface: (z, w) -> (2 z_surface - z, -w) below it
+__device__ __forceinline__ void reflect_surface(float& z, float& w, float z_surface) {
+    if (z < z_surface) {
+        z = 2.0f * z_surface - z;
+        w = -w;
+    }
+}
+
 }  // namespace glide

@@ -328,8 +328,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                         const float u = acc[0] * om + acc[3] * alpha;
                         const float vv = acc[1] * om + acc[4] * alpha;
                         const float w = acc[2] * om + acc[5] * alpha;
-                        const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(qy * DEG2RAD)), 0.05f);
-                        const float vx = u / m_lon, vy = vv / M_PER_DEG_LAT;
+                        const float vx = u / m_per_deg_lon(qy), vy = vv / M_PER_DEG_LAT;
                         if (stage == 0) {
                             qx = lon - hd * vx;
                             qy = lat - hd * vy;
@@ -431,10 +430,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
             const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
             const float umax = 4.0f * su, vmax = 4.0f * sv, wmax = 4.0f * sw;
-            const float au = expf(-sub_dt / tlu), av = expf(-sub_dt / tlv), aw = expf(-sub_dt / tlw);
-            const float ru = sqrtf(fmaxf(su2 * (1.0f - au * au), 0.0f));
-            const float rv = sqrtf(fmaxf(sv2 * (1.0f - av * av), 0.0f));
-            const float rw = sqrtf(fmaxf(sw2 * (1.0f - aw * aw), 0.0f));
+            const float au = ou_decay(sub_dt, tlu), av = ou_decay(sub_dt, tlv), aw = ou_decay(sub_dt, tlw);
+            const float ru = ou_amplitude(su2, au), rv = ou_amplitude(sv2, av), rw = ou_amplitude(sw2, aw);
             const int64_t nn = p.n;
             StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
             for (int it = 0; it < k; ++it) {
@@ -451,20 +448,16 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                 }
                 const float factor = 1.0f + (wp * wp) / sw_sq;
                 const float drift_w = factor * half_bwd + dens_bwd;
-                float un = (au * up + 0.0f * sub_dt) + ru * eu;
-                float vn = (av * vp + 0.0f * sub_dt) + rv * ev;
-                float wn = (aw * wp + drift_w * sub_dt) + rw * ew;
+                float un = ou_step(up, au, 0.0f * sub_dt, ru, eu);
+                float vn = ou_step(vp, av, 0.0f * sub_dt, rv, ev);
+                float wn = ou_step(wp, aw, drift_w * sub_dt, rw, ew);
                 wn = fminf(fmaxf(wn, -wmax), wmax);
                 un = fminf(fmaxf(un, -umax), umax);
                 vn = fminf(fmaxf(vn, -vmax), vmax);
-                z = z + (-wn) * sub_dt;
-                const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
-                lon = lon + ((-un) * sub_dt) / m_lon;
-                lat = lat + ((-vn) * sub_dt) / M_PER_DEG_LAT;
-                if (z < 0.0f) {
-                    z = 0.0f - z;
-                    wn = -wn;
-                }
+                z = displace_z(z, wn, sub_dt, -1.0f);
+                lon = displace_lon(lon, un, sub_dt, -1.0f, m_per_deg_lon(lat));
+                lat = displace_lat(lat, vn, sub_dt, -1.0f);
+                reflect_surface(z, wn, 0.0f);
                 up = un; vp = vn; wp = wn;
             }
 
@@ -479,13 +472,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                     e0 = rng.next();
                     e1 = rng.next();
                 }
-                const float am = expf(-delta / p.meander_T);
-                const float one_m = 1.0f - am * am;
-                const float umn = (am * um + 0.0f * delta) + sqrtf(fmaxf((m_su * m_su) * one_m, 0.0f)) * e0;
-                const float vmn = (am * vm + 0.0f * delta) + sqrtf(fmaxf((m_sv * m_sv) * one_m, 0.0f)) * e1;
-                const float m_lon = M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f);
-                lon = lon + ((-umn) * delta) / m_lon;
-                lat = lat + ((-vmn) * delta) / M_PER_DEG_LAT;
+                const float am = ou_decay(delta, p.meander_T);
+                const float umn = ou_step(um, am, 0.0f * delta, ou_amplitude(m_su * m_su, am), e0);
+                const float vmn = ou_step(vm, am, 0.0f * delta, ou_amplitude(m_sv * m_sv, am), e1);
+                lon = displace_lon(lon, umn, delta, -1.0f, m_per_deg_lon(lat));
+                lat = displace_lat(lat, vmn, delta, -1.0f);
                 um = umn; vm = vmn;
             }
             nonfinite |= !(isfinite(lon) && isfinite(lat) && isfinite(z) && isfinite(up) && isfinite(vp) &&

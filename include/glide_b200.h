@@ -176,6 +176,20 @@ typedef struct glide_convect_args {
     int32_t* n_moved;                        /* device counter (added to), may be NULL */
 } glide_convect_args;
 
+/* Exact-OU velocity update of the engine primitives (GPUEngine.update_langevin_velocity,
+ * src/lpdm/gpu_engine.py:345-398 with _ou_step_kernel :26-42). Each per-particle input
+ * is a device array [n] or, when NULL, the scalar beside it. */
+typedef struct glide_ou_args {
+    int64_t n;
+    float* w;                                   /* velocity [n], updated in place */
+    const float* t_l; float t_l_scalar;         /* Lagrangian timescale, s (> 0) */
+    const float* sigma2; float sigma2_scalar;   /* velocity variance, m^2/s^2 (>= 0) */
+    const float* dt; float dt_scalar;           /* step, s (> 0) */
+    const float* drift; float drift_scalar;     /* deterministic acceleration, m/s^2 (drift * dt added) */
+    const float* noise;                         /* standard normals [n], or NULL: drawn from (seed, counter) */
+    uint64_t seed; uint32_t counter;
+} glide_ou_args;
+
 /* --- library ------------------------------------------------------------------ */
 
 /* Version of this ABI (major * 10000 + minor * 100 + patch). */
@@ -185,8 +199,8 @@ int32_t glide_version(void);
 glide_status glide_last_error(char* buf, size_t len);
 
 /* sizeof of the ABI structs, in declaration order: glide_grid, glide_window_desc,
- * glide_step_sched, glide_footprint_grid, glide_step_args, glide_convect_args.
- * Lets a binding verify its struct layouts. Writes min(n, 6) values. */
+ * glide_step_sched, glide_footprint_grid, glide_step_args, glide_convect_args,
+ * glide_ou_args. Lets a binding verify its struct layouts. Writes min(n, 7) values. */
 glide_status glide_abi_struct_sizes(size_t* out, int32_t n);
 
 /* --- per-window met packing ------------------------------------------------------
@@ -224,6 +238,26 @@ glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t
 glide_status glide_reorder_scratch_bytes(int64_t n, size_t* bytes);
 glide_status glide_reorder_by_key(int64_t n, const uint8_t* work_key, int32_t* order, void* scratch,
                                   size_t scratch_bytes, void* stream);
+
+/* --- engine primitives -----------------------------------------------------------
+ * The per-substep updates of glide_step as separate launches on float32 device arrays,
+ * for engine-level callers and tests: GPUEngine.update_langevin_velocity,
+ * apply_vertical_turbulence, apply_horizontal_turbulence, reflect_surface and the stages
+ * of rk2_advect_backward (src/lpdm/gpu_engine.py:308-507). They run the same device
+ * functions as the fused kernel's substep loop. Positions use a stride (4 for the
+ * reference's (N, 4) particle tensor); dt is a device array [n] or, when NULL, dt_scalar;
+ * backward != 0 displaces by -velocity. */
+glide_status glide_ou_update(const glide_ou_args* args, void* stream);
+glide_status glide_displace_vertical(int64_t n, float* z, int64_t z_stride, const float* w, const float* dt,
+                                     float dt_scalar, int32_t backward, void* stream);
+glide_status glide_displace_horizontal(int64_t n, float* lon, float* lat, int64_t stride, const float* u,
+                                       const float* v, const float* dt, float dt_scalar, int32_t backward,
+                                       void* stream);
+/* (z, w) -> (2 z_surface - z, -w) where z < z_surface */
+glide_status glide_reflect_surface(int64_t n, float* z, int64_t z_stride, float* w, float z_surface, void* stream);
+/* out[i][0..3) = x[i][0..3) - h * v[i][0..3) (strides >= 3, in floats) */
+glide_status glide_rk2_stage(int64_t n, const float* x, int64_t x_stride, const float* v, int64_t v_stride, float h,
+                             float* out, int64_t out_stride, void* stream);
 
 /* --- footprint accumulation alone -----------------------------------------------
  * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the

@@ -31,8 +31,8 @@ def test_every_symbol_is_exported():
 
 
 def test_struct_layouts_match():
-    sizes = (C.c_size_t * 6)()
-    assert _abi.lib.glide_abi_struct_sizes(sizes, 6) == 0
+    sizes = (C.c_size_t * len(_abi.STRUCTS))()
+    assert _abi.lib.glide_abi_struct_sizes(sizes, len(_abi.STRUCTS)) == 0
     assert list(sizes) == [C.sizeof(s) for s in _abi.STRUCTS]
     assert _abi.lib.glide_version() >= 100
 
