@@ -46,7 +46,8 @@ SITE = (-5.0, 52.0)
 # algorithmic bytes per particle-step (met gathers 200 values x b + 86 B of state, footprint, flags)
 B_ALG = {"f32": 200 * 4 + 86, "bf16": 200 * 2 + 86, "f16": 200 * 2 + 86}
 METRIC = "particle-steps/s"
-CPU_SAMPLE_STEPS = 40  # outer steps of all particles per CPU sample (~5 s on 16 cores)
+CPU_SAMPLE_STEPS = 40  # outer steps of all particles per step of the reference arm (~5 s on 16 cores)
+CPU_BASELINE_STEPS = 120  # outer steps of all particles in the B200 arm's cpu_baseline sample (~15 s)
 
 
 def parse():
@@ -174,13 +175,14 @@ def measured_peak_hbm() -> tuple[float, str]:
 
 
 def prepare_cpu_sample(syn, cfg, n_particles: int) -> str:
-    """Saves the met window and particles the CPU sample needs (window [23 h, 24 h]) to an
-    .npz in shared memory for the worker processes. The sample is the second and
-    third outer steps of that window: per-window work (support stacks, convection)
+    """Saves the met window and particles the CPU sample needs to an .npz in shared
+    memory for the worker processes. The sample starts one outer step into the first
+    hour after the release hour, when every particle is released and active, so each
+    counted particle-step is computed; per-window work (support stacks, convection)
     is excluded from the CPU timing."""
     import tempfile
 
-    h = syn.window_index(cfg["cursor_start"] - timedelta(seconds=DT_S))
+    h = syn.window_index(cfg["batch_start"] - timedelta(seconds=DT_S))
     f0, f1 = syn.fields[h], syn.fields[h + 1]
     arrs = {f"w_{k}": np.stack([f0[k].cpu().numpy(), f1[k].cpu().numpy()]) for k in f0}
     arrs.update(height=syn.height_agl.cpu().numpy(), level=syn.levels, p_hpa=syn.pressure_level_hpa, lon=syn.lon,
@@ -188,7 +190,7 @@ def prepare_cpu_sample(syn, cfg, n_particles: int) -> str:
                 particles=cfg["particles"][:n_particles], rel_off=cfg["rel_off"][:n_particles],
                 win_end=cfg["win_end"][:n_particles],
                 batch_start=np.array(cfg["batch_start"].timestamp()),
-                cursor=np.array((cfg["cursor_start"] - timedelta(seconds=2 * DT_S)).timestamp()),
+                cursor=np.array((cfg["batch_start"] - timedelta(seconds=DT_S)).timestamp()),
                 terminus=np.array(cfg["terminus"].timestamp()))
     d = "/dev/shm" if os.path.isdir("/dev/shm") else None
     fd, path = tempfile.mkstemp(suffix=".npz", prefix="glide_cpu_", dir=d)
@@ -821,12 +823,12 @@ def main() -> None:
             workers = os.cpu_count() or 1
             path = prepare_cpu_sample(syn, cfg, args.particles)
             try:
-                rate, wall = cpu_oracle_rate(path, args.particles, CPU_SAMPLE_STEPS, workers)
+                rate, wall = cpu_oracle_rate(path, args.particles, CPU_BASELINE_STEPS, workers)
             finally:
                 os.unlink(path)
             line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": workers, "kind": "port",
-                                    "sample": f"{args.particles} particles x {CPU_SAMPLE_STEPS} outer steps "
-                                              f"mid-window (oracle port, {workers} processes, {wall:.1f} s)"}
+                                    "sample": f"{args.particles} particles x {CPU_BASELINE_STEPS} outer steps, all "
+                                              f"released (oracle port, {workers} processes, {wall:.1f} s)"}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
