@@ -221,8 +221,10 @@ class BatchRun:
                 self.footprint_out = torch.zeros(fp.shape, dtype=torch.float32, device=dev)
                 out = self.footprint_out
 
+                rows_out = out.view(fp.n_releases * fp.n_time_bins, -1)
+
                 def sink(r_idx, b_idx, slices):
-                    out[r_idx, b_idx] += slices
+                    rows_out.index_add_(0, r_idx * fp.n_time_bins + b_idx, slices.reshape(slices.shape[0], -1))
 
                 self.sink = sink
         self.z_edges = torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32), device=dev)
@@ -407,21 +409,27 @@ class BatchRun:
         lo = self._bins(j0)
         hi = self._bins(j1 - 1)
         nxt = self._bins(j1) if j1 < len(self.steps) else np.full_like(hi, np.inf)
-        r_idx, b_idx = [], []
-        for r in np.nonzero(np.isfinite(lo))[0]:
-            for b in range(int(lo[r]), int(hi[r]) + 1):
-                if b < nxt[r] and 0 <= b < fp.n_time_bins:
-                    r_idx.append(int(r))
-                    b_idx.append(b)
-        if not r_idx:
+        rel = np.nonzero(np.isfinite(lo))[0]
+        if rel.size == 0:
             return
-        dev = self.footprint.device
-        ri = torch.as_tensor(r_idx, dtype=torch.int64, device=dev)
-        bi = torch.as_tensor(b_idx, dtype=torch.int64, device=dev)
-        si = bi % fp.ring
-        slices = self.footprint[ri, si]
+        first, last = lo[rel].astype(np.int64), hi[rel].astype(np.int64)
+        span = np.maximum(last - first + 1, 0)
+        rep = np.repeat(np.arange(rel.size), span)  # (release, bin) pairs in release-major order
+        b_all = first[rep] + (np.arange(rep.size) - np.repeat(np.cumsum(span) - span, span))
+        keep = (b_all < nxt[rel][rep]) & (b_all >= 0) & (b_all < fp.n_time_bins)
+        if not keep.any():
+            return
+        idx = np.stack([rel[rep][keep], b_all[keep]]).astype(np.int64)
+        # through pinned memory: an asynchronous copy, so the host does not wait for the window
+        dev_idx = torch.from_numpy(idx).pin_memory().to(self.footprint.device, non_blocking=True)
+        ri, bi = dev_idx[0], dev_idx[1]
+        # the ring as rows of (release, slot) slices: index_select / index_fill_ enqueue
+        # without waiting for the device (a scalar index_put_ through advanced indexing does not)
+        rows = self.footprint.view(fp.n_releases * fp.ring, -1)
+        flat = ri * fp.ring + bi % fp.ring
+        slices = rows.index_select(0, flat).view((-1,) + tuple(self.footprint.shape[2:]))
         self.sink(ri, bi, slices)
-        self.footprint[ri, si] = 0.0
+        rows.index_fill_(0, flat, 0.0)
 
     def _convect_args(self, wf: WindowFields, j: int, scratch: torch.Tensor, n_particles: int) -> _abi.ConvectArgs:
         r, s, e = self.r, self.state, self.r.emanuel
@@ -472,6 +480,70 @@ class BatchRun:
         fp = self.footprint if self.r.footprint.ring == 0 else self.footprint_out
         return BatchOutput(self.state, fp, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
                            self.conv_log, status)
+
+
+class HostSliceStream:
+    """A ring-footprint sink (``BatchRunner(footprint_sink=...)``) that moves the
+    completed time-ago slices to pinned host memory on its own copy stream, so the
+    device-to-host traffic overlaps the following windows' steps instead of
+    delaying them. Each call copies the window's slices and their (release, bin)
+    indices into one of ``buffers`` alternating pinned buffers; ``on_host(r_idx,
+    b_idx, slices)`` (int64 numpy arrays and a pinned CPU tensor ``[k, Zb, Y, X]``,
+    valid during the call) runs on the host once a copy has landed: when its buffer
+    is needed again, or at ``drain()``. ``bytes_moved`` counts the slice bytes."""
+
+    def __init__(self, device, slice_shape: tuple, capacity: int, on_host: Callable | None = None,
+                 buffers: int = 2) -> None:
+        self.device = torch.device(device)
+        self.slice_shape = tuple(slice_shape)
+        self.on_host = on_host
+        self.copy_stream = torch.cuda.Stream(device=self.device)
+        self.bufs = [self._alloc(max(1, int(capacity))) for _ in range(max(1, buffers))]
+        self.pending: list = [None] * len(self.bufs)
+        self.next = 0
+        self.bytes_moved = 0
+
+    def _alloc(self, k: int) -> dict:
+        return {"slices": torch.empty((k,) + self.slice_shape, dtype=torch.float32).pin_memory(),
+                "idx": torch.empty((2, k), dtype=torch.int64).pin_memory()}
+
+    def _deliver(self, slot: int) -> None:
+        p = self.pending[slot]
+        if p is None:
+            return
+        done, k = p
+        done.synchronize()
+        self.pending[slot] = None
+        if self.on_host is not None:
+            buf = self.bufs[slot]
+            idx = buf["idx"][:, :k].numpy()
+            self.on_host(idx[0].copy(), idx[1].copy(), buf["slices"][:k])
+
+    def __call__(self, r_idx: torch.Tensor, b_idx: torch.Tensor, slices: torch.Tensor) -> None:
+        k = int(slices.shape[0])
+        slot = self.next
+        self.next = (self.next + 1) % len(self.bufs)
+        self._deliver(slot)
+        if k > self.bufs[slot]["slices"].shape[0]:
+            self.bufs[slot] = self._alloc(k)
+        buf = self.bufs[slot]
+        ready = torch.cuda.current_stream(self.device).record_event()
+        with torch.cuda.stream(self.copy_stream):
+            self.copy_stream.wait_event(ready)
+            buf["slices"][:k].copy_(slices, non_blocking=True)
+            buf["idx"][0, :k].copy_(r_idx, non_blocking=True)
+            buf["idx"][1, :k].copy_(b_idx, non_blocking=True)
+            for t in (slices, r_idx, b_idx):  # keep their memory until the copies have run
+                t.record_stream(self.copy_stream)
+            done = self.copy_stream.record_event()
+        self.pending[slot] = (done, k)
+        self.bytes_moved += slices.numel() * slices.element_size()
+
+    def drain(self) -> None:
+        """Waits for every copy in flight and hands it to ``on_host``."""
+        for i in range(len(self.bufs)):
+            slot = (self.next + i) % len(self.bufs)
+            self._deliver(slot)
 
 
 class BatchRunner:

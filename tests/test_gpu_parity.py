@@ -262,6 +262,39 @@ def test_ring_footprint_matches_dense(cuda_device):
     assert r.footprint.device_shape[1] == 2
 
 
+def test_ring_footprint_streamed_to_host(cuda_device):
+    """The ring's completed slices, moved to pinned host memory on a copy stream by
+    HostSliceStream (one-slice buffers, so every call waits for an earlier copy),
+    assemble on the host into the dense footprint."""
+    import dataclasses
+
+    from glide_b200.runtime import HostSliceStream
+
+    run = load_run("run_small")
+    dense = run_gpu(run, cuda_device).footprint.cpu().numpy()
+    host = np.zeros_like(dense)
+    calls = []
+
+    def on_host(r_idx, b_idx, slices):
+        calls.append(len(r_idx))
+        np.add.at(host, (r_idx, b_idx), slices.numpy())
+
+    r = runner_for(run, cuda_device)
+    r.footprint = dataclasses.replace(r.footprint, ring=2)
+    fp = r.footprint
+    to_host = HostSliceStream(cuda_device, (len(fp.z_edges) - 1, fp.n_y, fp.n_x), capacity=1, on_host=on_host)
+    r.footprint_sink = to_host
+    z = run.z
+    st = state_from(z["particles0"], z["rel_off"], z["win_end_off"], z["release_idx"], cuda_device)
+    out = r.start(st, batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
+                  cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]),
+                  dt_seconds=float(z["dt_s"])).run()
+    to_host.drain()
+    assert out.status == 0 and sum(calls) > 0
+    assert to_host.bytes_moved == sum(calls) * host[0, 0].size * 4
+    np.testing.assert_allclose(host, dense, rtol=1e-5, atol=1e-7)
+
+
 def test_launch_variants_give_the_same_results(cuda_device):
     """Every launch variant computes the same particles (the footprint may differ in
     atomic summation order only): the fast kernels at every shape against the general
