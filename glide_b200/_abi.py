@@ -17,7 +17,7 @@ LIB_PATH = Path(os.environ.get("GLIDE_B200_LIBRARY") or Path(__file__).resolve()
 GLIDE_OK = 0
 GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
 GLIDE_STATUS_NONFINITE_STATE, GLIDE_STATUS_BAD_ORDER = 1, 2
-GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 15, 16
+GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 63, 64
 
 vp = C.c_void_p
 

@@ -65,7 +65,10 @@ struct Surface {
     float blh, ustar, w_star, hL, L, f_abs;
 };
 
-struct Sig6 { float su, sv, sw, tlu, tlv, tlw; };
+struct Sig6 {
+    float su, sv, sw, tlu, tlv, tlw;
+    int branch;  // which closure branch produced them: 0 stable, 1 neutral, 2-4 unstable (T_Lw forms)
+};
 
 // sigma_w of the three regimes (no surface-layer override)
 __device__ __forceinline__ float sigma_w_bl(float z, const Surface& s) {
@@ -89,6 +92,7 @@ __device__ __forceinline__ Sig6 in_bl(float z, const Surface& s, float sw) {
     const float blh = s.blh, us = s.ustar;
     o.sw = sw;
     if (s.hL > 1.0f) {  // stable (hanna.py:192-222)
+        o.branch = 0;
         const float zoh = fminf(fmaxf(z / blh, 0.0f), 1.0f);
         const float om = fmaxf(1.0f - zoh, 0.0f);
         o.su = (2.0f * us) * om;
@@ -108,13 +112,17 @@ __device__ __forceinline__ Sig6 in_bl(float z, const Surface& s, float sw) {
         const float azl = fmaxf(zoh * (-hl), 0.0f);
         const float swc = fmaxf(o.sw, SIGMA_MIN);
         if (azl < 1.0f) {
+            o.branch = 2;
             o.tlw = (0.1f * z) / (swc * fmaxf(0.55f - 0.38f * azl, 1e-2f));
         } else if (zoh < 0.1f) {
+            o.branch = 3;
             o.tlw = (0.59f * z) / swc;
         } else {
+            o.branch = 4;
             o.tlw = ((0.15f * blh) / swc) * (1.0f - expf(-5.0f * zoh));
         }
     } else {  // neutral (hanna.py:225-252)
+        o.branch = 1;
         const float fa = s.f_abs;
         o.su = (2.0f * us) * expf(((-3.0f * fa) * z) / us);
         o.sv = o.sw;
@@ -295,7 +303,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
     // atomic) only when the cell (or time bin) changes, and at the end of the launch
     int64_t fp_cell = -1;
     float fp_acc = 0.0f;
-    int last_k = 1;         // substeps of the last physics step (work key)
+    int last_k = 1;         // work class of the last physics step (work key)
     bool last_active = false;
 
     for (int j = 0; j < p.n_steps; ++j) {
@@ -425,7 +433,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
             if (!(kq == kq)) k = 1;  // NaN
             const float sub_dt = delta / (float)k;
-            last_k = k;
+            // work class of this step (glide_step_args.work_key): the closure branch, whether
+            // the free-troposphere override applies, the substep count
+            last_k = 1 + (min(k, 6) - 1) + 6 * ((z_eval > S.blh ? 1 : 0) + 2 * col.branch);
 
             // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
             const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
@@ -546,7 +556,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
             if (alive) {
                 const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
                 if (!(GENERAL && p.active_mask) && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
-                else if (last_active) key = min(max(last_k, 1), GLIDE_WORK_PENDING - 1);
+                else if (last_active) key = last_k;
             }
             p.work_key[i] = (uint8_t)key;
         }

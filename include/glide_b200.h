@@ -37,8 +37,11 @@ enum {
     GLIDE_STATUS_BAD_ORDER = 1u << 1,       /* glide_step_args.order held an index outside [0, n) */
 };
 
-/* work classes written to glide_step_args.work_key */
-enum { GLIDE_WORK_DONE = 0, GLIDE_WORK_PENDING = 15, GLIDE_WORK_CLASSES = 16 };
+/* work classes written to glide_step_args.work_key: GLIDE_WORK_DONE, GLIDE_WORK_PENDING, or
+ * for a particle stepped in the launch's last step 1 + (min(k, 6) - 1) + 6 (ft + 2 branch),
+ * k its substeps, ft 1 above the boundary layer, branch the Hanna closure branch (0 stable,
+ * 1 neutral, 2-4 the unstable T_Lw forms): classes 1 .. 60 */
+enum { GLIDE_WORK_DONE = 0, GLIDE_WORK_PENDING = 63, GLIDE_WORK_CLASSES = 64 };
 
 /* Met grid geometry: GridInterpolationBounds (src/lpdm/gpu_engine.py:100-121). */
 typedef struct glide_grid {
@@ -152,8 +155,8 @@ typedef struct glide_step_args {
      * GLIDE_STATUS_BAD_ORDER; a repeated entry is not detected. */
     const int32_t* order;
     /* optional output, device [n] indexed by particle: the work class of the launch's last
-     * step, GLIDE_WORK_DONE (0, escaped or past the simulation length), 1 .. 14 (substeps
-     * taken, capped) or GLIDE_WORK_PENDING (15, alive but not yet released). */
+     * step (GLIDE_WORK_*): done (escaped or past the simulation length), pending (alive but
+     * not yet released), or the class of the branches and substep count it took. */
     uint8_t* work_key;
 } glide_step_args;
 
@@ -231,9 +234,10 @@ glide_status glide_step_launch_variant_info(int32_t v, int32_t* threads, int32_t
  * No counterpart in the reference (its static path runs every particle through the
  * same tensor ops). Builds order[0 .. n) for glide_step_args.order from a work_key
  * written by the previous launch: descending work class (GLIDE_WORK_PENDING first,
- * then 14 .. 1 substeps, GLIDE_WORK_DONE last), stable within a class, so that the
- * lanes of a warp run the same number of substeps and the longest warps start first.
- * Keys above 15 count as 15. Three launches on `stream`, no synchronisation; scratch
+ * GLIDE_WORK_DONE last), stable within a class, so that the lanes of a warp take the
+ * same closure branches and the same number of substeps, and finished particles fill
+ * whole warps. Keys above GLIDE_WORK_PENDING count as it. Three launches on `stream`,
+ * no synchronisation; scratch
  * is device memory of glide_reorder_scratch_bytes(n) bytes. n <= INT32_MAX. */
 glide_status glide_reorder_scratch_bytes(int64_t n, size_t* bytes);
 glide_status glide_reorder_by_key(int64_t n, const uint8_t* work_key, int32_t* order, void* scratch,

@@ -33,15 +33,16 @@ def _reorder(keys: np.ndarray, device) -> np.ndarray:
 
 
 def _expected(keys: np.ndarray) -> np.ndarray:
-    return np.argsort(15 - np.minimum(keys.astype(np.int64), 15), kind="stable").astype(np.int32)
+    top = 63  # GLIDE_WORK_PENDING: the largest class
+    return np.argsort(top - np.minimum(keys.astype(np.int64), top), kind="stable").astype(np.int32)
 
 
 @pytest.mark.parametrize("n", [1, 31, 1023, 1024, 1025, 4096 + 77, 200_001])
 def test_reorder_is_a_stable_descending_sort(cuda_device, n):
     rng = np.random.default_rng(n)
-    keys = rng.integers(0, 7, n).astype(np.uint8)
-    keys[rng.random(n) < 0.1] = 15
-    keys[rng.random(n) < 0.01] = 200  # counts as 15
+    keys = rng.integers(0, 61, n).astype(np.uint8)
+    keys[rng.random(n) < 0.1] = 63
+    keys[rng.random(n) < 0.01] = 200  # counts as 63
     np.testing.assert_array_equal(_reorder(keys, cuda_device), _expected(keys))
 
 
@@ -109,9 +110,13 @@ def test_work_keys_and_bad_order(cuda_device):
     alive = st.alive.cpu().numpy().astype(bool)
     ms = int(z["max_substeps"])
     assert np.all(keys[~alive] == _abi.GLIDE_WORK_DONE)
-    live = keys[alive]
-    assert np.all(((live >= 1) & (live <= ms)) | (live == _abi.GLIDE_WORK_PENDING))
-    assert np.any((live >= 1) & (live <= ms))
+    live = keys[alive].astype(np.int64)
+    stepped = (live >= 1) & (live <= 60)
+    assert np.all(stepped | (live == _abi.GLIDE_WORK_PENDING))
+    assert np.any(stepped)
+    k = (live[stepped] - 1) % 6 + 1  # substeps (capped at 6)
+    branch = (live[stepped] - 1) // 12
+    assert np.all(k <= ms) and np.all(branch <= 4)
 
     # one single-step launch of the next window through a corrupted permutation
     k = br.next_window
