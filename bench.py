@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="use launch variant 0 instead of tuning")
     ap.add_argument("--no-reorder", action="store_true", help="step particles in index order (no work-class sort)")
     ap.add_argument("--no-pipeline", action="store_true", help="prepare each window inline (no side stream)")
+    ap.add_argument("--steps-per-launch", type=int, default=None,
+                    help="outer steps per step-kernel launch with --no-autotune (default: a whole window)")
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
@@ -709,13 +711,14 @@ def main() -> None:
     if args.warmup + args.steps > n_windows_total:
         raise SystemExit(f"warmup + steps must be <= {n_windows_total} windows (the 24 h job)")
 
-    tuned = {"variant": 0, "times_ms": {}}
+    tuned = {"variant": 0, "steps_per_launch": args.steps_per_launch, "times_ms": {}}
 
     def make_runner(provider):
         r = BatchRunner(grid=grid, window_provider=provider, hanna=cfg["hanna"], footprint=cfg["footprint"],
                         domain=cfg["domain"], emanuel=cfg["emanuel"], met_dtype=args.met, device=dev,
                         seed=1234 + rank, pipeline=not args.no_pipeline)
         r.launch_variant = tuned["variant"]
+        r.steps_per_launch = tuned["steps_per_launch"]
         r.reorder = not args.no_reorder
         return r
 
@@ -750,6 +753,15 @@ def main() -> None:
         return rc
 
     abi.lib.glide_step = timed_step
+    real_reorder = abi.lib.glide_reorder_by_key
+    reorders = [0]
+
+    def counted_reorder(*a):  # three kernels per call
+        if record_kernels:
+            reorders[0] += 1
+        return real_reorder(*a)
+
+    abi.lib.glide_reorder_by_key = counted_reorder
     record_kernels = False
     run = runner.start(fresh_state(), **kw)
     for _ in range(args.warmup):
@@ -809,14 +821,18 @@ def main() -> None:
                        "max_substeps": 6, "step": "one met window (pack + convection + fused steps)",
                        "l2": "flushed (256 MB write) before every timed step; met bricks 440 MB > L2",
                        "parallelism": f"replicas x{world}", "launch_variant": tuned["variant"],
-                       "particle_order": "identity" if args.no_reorder else "work class, rebuilt per window",
-                       "autotune_ms_per_window": {str(k): round(v, 3) for k, v in tuned["times_ms"].items()}},
+                       "steps_per_launch": tuned["steps_per_launch"] or "window",
+                       "particle_order": "identity" if args.no_reorder else "work class, rebuilt before every launch",
+                       "autotune_ms_per_window": {str(k): round(v, 3) for k, v in tuned["times_ms"].items()},
+                       "autotune_steps_per_launch_ms": {str(k or "window"): round(v, 3)
+                                                        for k, v in tuned.get("steps_times_ms", {}).items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "kernel": "step_kernel", "bytes_per_particle_step": B_ALG[args.met],
                          "kernel_time_share": t_kernel / t_dev},
             "clocks": clk,
-            "gpu_launches": n_kernel_launches + (6 if args.no_reorder else 9) * args.steps,
+            # step launches + 3 per particle-order rebuild + per window: 2 packing, 2 column, 1 redistribution
+            "gpu_launches": n_kernel_launches + 3 * reorders[0] + 5 * args.steps,
             "status": status,
         }
         if e2e is not None:

@@ -254,7 +254,8 @@ class BatchRun:
         # particle ordering by work class (glide_reorder_by_key): each window's launches step
         # the particles in the order built from the work keys of the previous window
         self.order = self.work_key = self.reorder_scratch = None
-        self.keys_valid = False
+        self.keys_valid = False  # work_key holds the keys of a launch
+        self.order_valid = False  # order holds a permutation built from such keys
         if runner.reorder and state.n > 0:
             nb = C.c_size_t()
             _abi.check(_abi.lib.glide_reorder_scratch_bytes(state.n, C.byref(nb)), "glide_reorder_scratch_bytes")
@@ -267,7 +268,9 @@ class BatchRun:
         return self.next_window >= len(self.windows)
 
     def _step_args(self, packed: PackedWindow, j0: int, n_steps: int, phys_begin: int, post_begin: int,
-                   noise) -> _abi.StepArgs:
+                   noise, noise_row: int = 0) -> _abi.StepArgs:
+        """Arguments of one ``glide_step`` launch of steps [j0, j0 + n_steps); ``noise_row``
+        is j0's row in the window's injected noise buffers."""
         r, s = self.r, self.state
         h = r.hanna
         a = _abi.StepArgs()
@@ -290,8 +293,8 @@ class BatchRun:
         a.n_steps, a.phys_begin, a.post_begin = n_steps, phys_begin, post_begin
         if noise is not None:
             sub, mea = noise
-            a.noise_substep = sub.data_ptr()
-            a.noise_meander = None if mea is None else mea.data_ptr()
+            a.noise_substep = sub[noise_row].data_ptr()
+            a.noise_meander = None if mea is None else mea[noise_row].data_ptr()
         a.seed = r.seed
         a.footprint = self.footprint.data_ptr()
         fp = r.footprint
@@ -307,9 +310,32 @@ class BatchRun:
         a.status = self.status.data_ptr()
         a.launch_variant = r.launch_variant
         if self.work_key is not None:
-            a.order = self.order.data_ptr() if self.keys_valid else None
+            a.order = self.order.data_ptr() if self.order_valid else None
             a.work_key = self.work_key.data_ptr()
         return a
+
+    def _reorder(self, sh) -> None:
+        """Rebuild the particle order from the work keys of the last launch."""
+        if self.keys_valid:
+            _abi.check(_abi.lib.glide_reorder_by_key(self.state.n, self.work_key.data_ptr(), self.order.data_ptr(),
+                                                     self.reorder_scratch.data_ptr(), self.reorder_scratch.numel(),
+                                                     sh), "glide_reorder_by_key")
+            self.order_valid = True
+
+    def _launch_range(self, packed: PackedWindow, j0: int, j1: int, phys_skip: int, noise, sh) -> None:
+        """The window's steps [j0, j1) in launches of ``steps_per_launch`` steps (all in one
+        when unset), the particle order rebuilt between launches; the first launch leaves
+        out the physics of its first ``phys_skip`` steps (already run before convection)."""
+        per = self.r.steps_per_launch or (j1 - j0)
+        j = j0
+        while j < j1:
+            c = min(per, j1 - j)
+            if j > j0:
+                self._reorder(sh)
+            a = self._step_args(packed, j, c, phys_skip if j == j0 else 0, 0, noise, noise_row=j - j0)
+            _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+            self.keys_valid = self.work_key is not None
+            j += c
 
     def _prepare(self, k: int) -> None:
         """Per-window work that depends only on met: fetch the window, pack its bricks
@@ -365,20 +391,15 @@ class BatchRun:
         sh = stream_handle(main)
         n = j1 - j0
         with torch.cuda.stream(main):
-            if self.keys_valid:
-                _abi.check(_abi.lib.glide_reorder_by_key(self.state.n, self.work_key.data_ptr(), self.order.data_ptr(),
-                                                         self.reorder_scratch.data_ptr(),
-                                                         self.reorder_scratch.numel(), sh), "glide_reorder_by_key")
+            self._reorder(sh)
             if r.emanuel is not None:
                 a = self._step_args(packed, j0, 1, 0, 1, noise)
                 _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+                self.keys_valid = self.work_key is not None
                 self._redistribute(wf, j0, scratch, main)
-                a = self._step_args(packed, j0, n, 1, 0, noise)
-                _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
+                self._launch_range(packed, j0, j1, 1, noise, sh)
             else:
-                a = self._step_args(packed, j0, n, 0, 0, noise)
-                _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
-            self.keys_valid = self.work_key is not None
+                self._launch_range(packed, j0, j1, 0, noise, sh)
             done = torch.cuda.Event()
             done.record(main)
             self.slot_free[k % 2 if self.pipelined else 0] = done
@@ -579,6 +600,7 @@ class BatchRunner:
         self.pipeline = bool(pipeline)
         self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
         self.reorder = True  # group particles by work class each window (results do not depend on it)
+        self.steps_per_launch: int | None = None  # split each window into launches of this many steps
         self._step_stream = None
         self._slots: list[PackedWindow | None] = [None, None]
 
