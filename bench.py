@@ -406,8 +406,9 @@ def run_serving(args) -> None:
     site among 56, release time uniform in 48 h, particles log-uniform in
     [1e3, 5e4], backward duration uniform in [6, 120] h, dt 30 s, BF16 met with all
     169 windows resident; 60 GB budget for particle state and footprints. Reports
-    throughput and p50/p90/p99 end-to-end latency, and the same requests run one at a
-    time (no overlap) for comparison."""
+    throughput and p50/p90/p99 end-to-end latency; then the capacity with the same
+    requests submitted at once, and the same requests run one at a time (no overlap)
+    for comparison."""
     import dataclasses
 
     import torch
@@ -449,6 +450,14 @@ def run_serving(args) -> None:
             "active_particle_steps_per_s": aps / wall, "peak_active": server.stats.peak_active,
             "peak_state_bytes": server.stats.peak_bytes, "resident_packed_bytes": server.resident.nbytes,
             "pack_s": t_pack, "dtype": kw["met_dtype"], "clocks": clocks.summary()}
+    # capacity: the same requests all submitted at once
+    sat = FootprintServer(max_active=args.max_active, n_streams=16, **kw)
+    t = time.perf_counter()
+    sat_res = sat.serve([dataclasses.replace(r) for r in reqs], realtime=False)
+    sat_wall = time.perf_counter() - t
+    line["saturated"] = {"footprints_per_s": len(sat_res) / sat_wall, "wall_s": sat_wall,
+                         "active_particle_steps_per_s": sum(r.active_particle_steps for r in sat_res) / sat_wall,
+                         "peak_active": sat.stats.peak_active}
     if not args.no_sequential:
         seq = FootprintServer(max_active=1, n_streams=1, **kw)
         t = time.perf_counter()

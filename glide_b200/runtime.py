@@ -123,17 +123,26 @@ class ParticleState:
         if p.dim() != 2 or p.shape[1] != 4:
             raise ValueError("particles must have shape (N, 4)")
         n = p.shape[0]
-        p = p.to(device)
+        p = _upload(p, device)
         z = torch.zeros(n, dtype=torch.float32, device=device)
         return cls(p[:, 0].contiguous(), p[:, 1].contiguous(), p[:, 2].contiguous(), p[:, 3].contiguous(),
                    z.clone(), z.clone(), z.clone(), z.clone(), z.clone(),
-                   torch.as_tensor(rel_off, dtype=torch.float32).to(device),
-                   torch.as_tensor(win_end_off, dtype=torch.float32).to(device),
-                   torch.as_tensor(release_idx).to(device=device, dtype=torch.int32),
+                   _upload(torch.as_tensor(rel_off, dtype=torch.float32), device),
+                   _upload(torch.as_tensor(win_end_off, dtype=torch.float32), device),
+                   _upload(torch.as_tensor(release_idx), device).to(dtype=torch.int32),
                    torch.ones(n, dtype=torch.uint8, device=device))
 
     def particles(self) -> torch.Tensor:
         return torch.stack([self.lon, self.lat, self.z, self.weight], dim=1)
+
+
+def _upload(t: torch.Tensor, device) -> torch.Tensor:
+    """Host tensor -> device through pinned memory, asynchronous on the current stream
+    (a pageable copy would wait for the stream's earlier work); device tensors pass."""
+    device = torch.device(device)
+    if t.device == device or device.type != "cuda":
+        return t.to(device)
+    return t.contiguous().pin_memory().to(device, non_blocking=True)
 
 
 @dataclass
@@ -150,10 +159,76 @@ def hour_floor(t: datetime) -> datetime:
     return t.astimezone(UTC).replace(minute=0, second=0, microsecond=0)
 
 
+_EPOCH = datetime(1970, 1, 1, tzinfo=UTC)
+_US = timedelta(microseconds=1)
+_HOUR_US = 3_600_000_000
+
+
+class StepPlans:
+    """The cursor walk as arrays — cursor and hour instants in integer microseconds
+    since the epoch, float64 cursor offsets, step lengths and RK2 weights — so a
+    batch of thousands of steps is planned without a Python loop. Indexing gives
+    ``StepPlan`` records; slicing gives a shorter ``StepPlans``."""
+
+    def __init__(self, cursor_us: np.ndarray, cursor_off: np.ndarray, delta: np.ndarray, hour_us: np.ndarray,
+                 alpha: np.ndarray, tz) -> None:
+        self.cursor_us, self.cursor_off, self.delta = cursor_us, cursor_off, delta
+        self.hour_us, self.alpha, self.tz = hour_us, alpha, tz
+
+    def __len__(self) -> int:
+        return int(self.cursor_us.shape[0])
+
+    def __getitem__(self, k):
+        if isinstance(k, slice):
+            return StepPlans(self.cursor_us[k], self.cursor_off[k], self.delta[k], self.hour_us[k], self.alpha[k],
+                             self.tz)
+        cursor = (_EPOCH + int(self.cursor_us[k]) * _US).astimezone(self.tz)
+        return StepPlan(cursor, float(self.cursor_off[k]), float(self.delta[k]), _EPOCH + int(self.hour_us[k]) * _US,
+                        float(self.alpha[k]))
+
+    def __iter__(self):
+        return (self[k] for k in range(len(self)))
+
+
 def plan_steps(batch_start: datetime, cursor_start: datetime, cursor_terminus: datetime,
-               dt_seconds: float) -> list[StepPlan]:
+               dt_seconds: float) -> StepPlans | list[StepPlan]:
     """The cursor walk of main.py:1383-1389, 1610 with the alpha of main.py:916-919
-    for hourly windows [hour, hour + 1 h]."""
+    for hourly windows [hour, hour + 1 h]: steps of ``dt_seconds`` back from
+    ``cursor_start`` while the cursor is after ``cursor_terminus``, the last one cut
+    to end on it. Timezone-aware instants are planned with numpy in exact integer
+    microseconds, reproducing ``datetime`` arithmetic (step lengths rounded to the
+    microsecond as ``timedelta`` rounds them); naive ones step by step."""
+    if cursor_start.tzinfo is None or cursor_terminus.tzinfo is None or batch_start.tzinfo is None:
+        return _plan_steps_loop(batch_start, cursor_start, cursor_terminus, dt_seconds)
+    dt = float(dt_seconds)
+    dt_us = timedelta(seconds=dt) // _US
+    if dt_us <= 0:
+        raise ValueError("dt_seconds must be positive")
+    t0 = (cursor_start - _EPOCH) // _US
+    term = (cursor_terminus - _EPOCH) // _US
+    b = batch_start.timestamp()
+    if t0 <= term:
+        z = np.zeros(0)
+        return StepPlans(np.zeros(0, np.int64), z, z, np.zeros(0, np.int64), z, cursor_start.tzinfo)
+    # full steps while the remaining span exceeds dt (as the float comparison of min() sees it)
+    n_max = (t0 - term) // dt_us + 2
+    j = np.arange(n_max, dtype=np.int64)
+    remain_s = (t0 - term - j * dt_us) / 1e6
+    full = remain_s > dt
+    n_full = int(np.argmin(full)) if not full.all() else n_max
+    cursor_us = t0 - np.arange(n_full + 1, dtype=np.int64) * dt_us
+    delta = np.full(n_full + 1, dt)
+    delta[n_full] = remain_s[n_full]
+    t_s = cursor_us / 1e6
+    hour_us = cursor_us - np.mod(cursor_us, _HOUR_US)
+    ts = hour_us / 1e6
+    te = (hour_us + _HOUR_US) / 1e6
+    alpha = np.clip((t_s - 0.5 * delta - ts) / np.maximum(1.0, te - ts), 0.0, 1.0)
+    return StepPlans(cursor_us, t_s - b, delta, hour_us, alpha, cursor_start.tzinfo)
+
+
+def _plan_steps_loop(batch_start: datetime, cursor_start: datetime, cursor_terminus: datetime,
+                     dt_seconds: float) -> list[StepPlan]:
     steps = []
     t = cursor_start
     b = batch_start.timestamp()
@@ -167,12 +242,36 @@ def plan_steps(batch_start: datetime, cursor_start: datetime, cursor_terminus: d
     return steps
 
 
-def schedule_array(steps: list[StepPlan]) -> np.ndarray:
+def schedule_array(steps) -> np.ndarray:
     """``glide_step_sched`` records (float32 cursor offset, delta, alpha; int32 index)."""
     rec = np.zeros(len(steps), dtype=np.dtype([("c", "<f4"), ("d", "<f4"), ("a", "<f4"), ("i", "<i4")]))
+    if isinstance(steps, StepPlans):
+        rec["c"], rec["d"], rec["a"] = steps.cursor_off, steps.delta, steps.alpha
+        rec["i"] = np.arange(len(steps), dtype=np.int32)
+        return rec
     for k, s in enumerate(steps):
         rec[k] = (np.float32(s.cursor_off), np.float32(s.delta), np.float32(s.alpha), k)
     return rec
+
+
+def window_ranges(steps) -> list[tuple[int, int]]:
+    """Runs [k, e) of consecutive steps in the same hourly window."""
+    if isinstance(steps, StepPlans):
+        h = steps.hour_us
+        if h.size == 0:
+            return []
+        cuts = np.flatnonzero(h[1:] != h[:-1]) + 1
+        edges = [0, *cuts.tolist(), int(h.size)]
+        return list(zip(edges[:-1], edges[1:]))
+    out = []
+    k = 0
+    while k < len(steps):
+        e = k
+        while e < len(steps) and steps[e].hour == steps[k].hour:
+            e += 1
+        out.append((k, e))
+        k = e
+    return out
 
 
 @dataclass
@@ -195,7 +294,7 @@ class BatchRun:
         self.steps = steps
         self.sim_length_s = float(sim_length_s)
         dev = runner.device
-        self.sched_dev = torch.from_numpy(schedule_array(steps).view(np.uint8).copy()).to(dev)
+        self.sched_dev = _upload(torch.from_numpy(schedule_array(steps).view(np.uint8).copy()), dev)
         self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -229,14 +328,7 @@ class BatchRun:
                 self.sink = sink
         self.z_edges = torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32), device=dev)
         # windows = runs of consecutive steps with the same hour
-        self.windows: list[tuple[int, int]] = []
-        k = 0
-        while k < len(steps):
-            e = k
-            while e < len(steps) and steps[e].hour == steps[k].hour:
-                e += 1
-            self.windows.append((k, e))
-            k = e
+        self.windows: list[tuple[int, int]] = window_ranges(steps)
         self.next_window = 0
         self.conv_log: list = []
         # per-window preparation, double-buffered when pipelined (bricks and column of

@@ -92,6 +92,7 @@ class _Active:
     admitted_s: float
     done_event: torch.cuda.Event | None = None
     issued_all: bool = False
+    host: dict | None = None  # pinned copies of the results, valid once done_event has completed
 
 
 @dataclass
@@ -183,16 +184,30 @@ class FootprintServer:
         self.bytes_in_use += nb
         self.stats.admitted += 1
 
-    def _finish(self, a: _Active, now_s: float) -> FootprintResult:
+    def _collect(self, a: _Active) -> None:
+        """Queue the request's reductions and their copies to pinned host memory behind
+        its last window, then its done event: nothing here waits for the device."""
         run = a.run
+        n = len(run.steps)
         with torch.cuda.stream(a.stream):
             fp = run.footprint[0]
-            totals = fp.sum(dim=(1, 2, 3), dtype=torch.float64).cpu().numpy()
-            n = len(run.steps)
-            esc = int(run.esc[:n].sum().item())
-            act = int(run.act[:n].to(torch.int64).sum().item())
-            host = fp.cpu() if self.keep else None
-        return FootprintResult(a.req.request_id, host, totals, esc, n, act, a.req.arrival_s, a.admitted_s, now_s)
+            counts = torch.stack([run.esc[:n].to(torch.int64).sum(), run.act[:n].to(torch.int64).sum()])
+            host = {"totals": torch.empty(fp.shape[0], dtype=torch.float64).pin_memory(),
+                    "counts": torch.empty(2, dtype=torch.int64).pin_memory()}
+            host["totals"].copy_(fp.sum(dim=(1, 2, 3), dtype=torch.float64), non_blocking=True)
+            host["counts"].copy_(counts, non_blocking=True)
+            if self.keep:
+                host["footprint"] = torch.empty(fp.shape, dtype=fp.dtype).pin_memory()
+                host["footprint"].copy_(fp, non_blocking=True)
+            a.done_event = torch.cuda.Event()
+            a.done_event.record(a.stream)
+        a.host = host
+
+    def _finish(self, a: _Active, now_s: float) -> FootprintResult:
+        h = a.host  # the done event has completed: the pinned copies are final
+        esc, act = (int(v) for v in h["counts"].tolist())
+        return FootprintResult(a.req.request_id, h.get("footprint"), h["totals"].numpy(), esc, len(a.run.steps), act,
+                               a.req.arrival_s, a.admitted_s, now_s)
 
     # -- the scheduling loop ------------------------------------------------------
 
@@ -220,8 +235,7 @@ class FootprintServer:
                 self.stats.windows_issued += 1
                 if a.run.done:
                     a.issued_all = True
-                    a.done_event = torch.cuda.Event()
-                    a.done_event.record(a.stream)
+                    self._collect(a)
         finished = []
         keep = []
         for a in self.active:
