@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="use launch variant 0 instead of tuning")
     ap.add_argument("--no-reorder", action="store_true", help="step particles in index order (no work-class sort)")
     ap.add_argument("--no-pipeline", action="store_true", help="prepare each window inline (no side stream)")
+    ap.add_argument("--separate-convection", action="store_true",
+                    help="convection in its own kernel between two step launches (not fused)")
     ap.add_argument("--steps-per-launch", type=int, default=None,
                     help="outer steps per step-kernel launch with --no-autotune (default: a whole window)")
     ap.add_argument("--sites", type=int, default=56)
@@ -728,6 +730,7 @@ def main() -> None:
                         seed=1234 + rank, pipeline=not args.no_pipeline)
         r.launch_variant = tuned["variant"]
         r.steps_per_launch = tuned["steps_per_launch"]
+        r.fuse_convection = not args.separate_convection
         r.reorder = not args.no_reorder
         return r
 

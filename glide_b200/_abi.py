@@ -60,7 +60,8 @@ class StepArgs(C.Structure):
                 ("fp", FootprintGrid), ("dom_lon_min", C.c_double), ("dom_lon_max", C.c_double),
                 ("dom_lat_min", C.c_double), ("dom_lat_max", C.c_double), ("dom_alt_max", C.c_double),
                 ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32),
-                ("order", vp), ("work_key", vp)]
+                ("order", vp), ("work_key", vp), ("conv_column", vp), ("conv_step", C.c_int32),
+                ("conv_nz", C.c_int32), ("conv_uniforms", vp), ("conv_moved", vp)]
 
 
 class ConvectArgs(C.Structure):

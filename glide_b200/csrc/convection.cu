@@ -18,6 +18,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "convect.cuh"
 #include "glide_internal.h"
 
 namespace glide {
@@ -269,9 +270,8 @@ __global__ void column_build_kernel(const ConvDev d) {
 
 __global__ void redistribute_kernel(const ConvDev d) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const double* S = d.scratch;
     int moved = 0;
-    if (i < d.n && S[0] != 0.0) {
+    if (i < d.n && d.scratch[0] != 0.0) {
         bool active;
         if (d.active_mask) active = d.active_mask[i] != 0;
         else {
@@ -279,35 +279,16 @@ __global__ void redistribute_kernel(const ConvDev d) {
             active = (!d.alive || d.alive[i]) && rel >= d.sched.cursor_off && (rel - d.sim_length) <= d.sched.cursor_off;
         }
         if (active) {
-            const int n = d.nz;
-            const double* h = S + 8 + 3 * n;
-            const double* cum = S + 8 + 4 * n;
-            const float zf = d.z[i * d.zs];
-            const double z = (double)zf;
-            int lo = 0, hi = n;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (h[mid] < z) lo = mid + 1; else hi = mid;
-            }
-            const int iu = min(max(lo, 1), n - 1), il = iu - 1;
-            const int host = ((z - h[il]) < (h[iu] - z)) ? il : iu;
             double u1, u2;
             if (d.uniforms) {
                 u1 = (double)d.uniforms[i];
                 u2 = (double)d.uniforms[d.n + i];
             } else {
-                const U4 r = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)d.sched.step_index,
-                                              STREAM_CONVECTION}, d.seed_lo, d.seed_hi);
-                u1 = (double)u01(r.x);
-                u2 = (double)u01(r.y);
+                convection_uniforms(i, (uint32_t)d.sched.step_index, d.seed_lo, d.seed_hi, u1, u2);
             }
-            const double* row = cum + (int64_t)host * n;
-            int dest = 0;
-            for (int c = 0; c < n; ++c) dest += (row[c] < u1) ? 1 : 0;
-            dest = min(dest, n - 1);
-            if (dest != host) {
-                const double zl = h[max(dest - 1, 0)], zh = h[dest];
-                d.z[i * d.zs] = (float)(zl + u2 * (zh - zl));
+            float z = d.z[i * d.zs];
+            if (convect_particle(d.scratch, d.nz, z, u1, u2)) {
+                d.z[i * d.zs] = z;
                 moved = 1;
             }
         }

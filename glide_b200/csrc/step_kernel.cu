@@ -20,6 +20,7 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "convect.cuh"
 #include "glide_internal.h"
 
 namespace glide {
@@ -55,6 +56,7 @@ struct StepDev {
     int32_t* esc; int32_t* act;
     uint32_t* status;
     const int32_t* order; uint8_t* work_key;
+    const double* conv_column; int conv_step, conv_nz; const float* conv_uniforms; int32_t* conv_moved;
 };
 
 // ---------------------------------------------------------------------------
@@ -493,6 +495,24 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
                            isfinite(wp));
         }
 
+        // --- the window's convection, fused: after the physics of its first step, before
+        // that step's footprint and escape kill (main.py:1446-1458, emanuel.py:772-805)
+        if (p.conv_column && j == p.conv_step) {
+            bool moved = false;
+            if (active) {
+                double u1, u2;
+                if (GENERAL && p.conv_uniforms) {
+                    u1 = (double)p.conv_uniforms[i];
+                    u2 = (double)p.conv_uniforms[p.n + i];
+                } else {
+                    convection_uniforms(i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi, u1, u2);
+                }
+                moved = convect_particle(p.conv_column, p.conv_nz, z, u1, u2);
+            }
+            const int n_mv = __popc(__ballot_sync(0xffffffffu, moved));
+            if (p.conv_moved && lane == 0 && n_mv) atomicAdd(p.conv_moved, n_mv);
+        }
+
         if (j >= p.post_begin) {
             // --- time-ago bin (main.py:1459-1465) and footprint (footprint_gridder.py:154-197)
             bool valid = false;
@@ -617,6 +637,10 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (a->launch_variant < 0 || a->launch_variant >= kNumVariants)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", a->launch_variant);
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
+    if (a->conv_column && (a->conv_nz < 2 || a->conv_step < 0 || a->conv_step >= a->n_steps))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: fused convection needs conv_nz >= 2 and 0 <= conv_step < n_steps");
+    if (a->conv_column && ((uintptr_t)a->conv_column & 7u))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: conv_column must be 8-byte aligned");
     if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
                          a->fp.n_time_bins < 1 || a->fp.n_releases < 1 || a->fp.ring < 0))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: invalid footprint grid");
@@ -657,8 +681,10 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.esc = a->escaped_per_step; d.act = a->active_per_step;
     d.status = a->status;
     d.order = a->order; d.work_key = a->work_key;
+    d.conv_column = static_cast<const double*>(a->conv_column); d.conv_step = a->conv_step; d.conv_nz = a->conv_nz;
+    d.conv_uniforms = a->conv_uniforms; d.conv_moved = a->conv_moved;
     cudaStream_t s = (cudaStream_t)stream;
-    const bool general = d.sl_override || d.noise_sub || d.noise_mea || d.active_mask;
+    const bool general = d.sl_override || d.noise_sub || d.noise_mea || d.active_mask || d.conv_uniforms;
     const int variant = general ? kNumShapes : a->launch_variant;
     switch (a->met_dtype) {
         case GLIDE_MET_F32: return launch_step<float>(d, s, variant);

@@ -414,10 +414,24 @@ class BatchRun:
                                                      sh), "glide_reorder_by_key")
             self.order_valid = True
 
-    def _launch_range(self, packed: PackedWindow, j0: int, j1: int, phys_skip: int, noise, sh) -> None:
+    def _fused_convection(self, wf: WindowFields, j: int, scratch: torch.Tensor) -> dict:
+        """Fields of the window's convection fused into its first launch (at its first
+        step) against the column prebuilt on the prep stream."""
+        r, s = self.r, self.state
+        moved = torch.zeros(1, dtype=torch.int32, device=r.device)
+        u = r.conv_uniform_provider(j) if r.conv_uniform_provider is not None else None
+        if u is not None and (tuple(u.shape) != (2, s.n) or u.dtype != torch.float32 or not u.is_contiguous()):
+            raise ValueError(f"injected convection uniforms must be contiguous float32 (2, {s.n})")
+        self.conv_log.append((wf.time_start, moved))
+        return {"conv_column": scratch.data_ptr(), "conv_nz": r.grid.shape[0], "conv_moved": moved.data_ptr(),
+                "conv_uniforms": None if u is None else u.data_ptr(), "keep": u}
+
+    def _launch_range(self, packed: PackedWindow, j0: int, j1: int, phys_skip: int, noise, sh,
+                      conv: dict | None = None) -> None:
         """The window's steps [j0, j1) in launches of ``steps_per_launch`` steps (all in one
         when unset), the particle order rebuilt between launches; the first launch leaves
-        out the physics of its first ``phys_skip`` steps (already run before convection)."""
+        out the physics of its first ``phys_skip`` steps (already run before convection),
+        and applies ``conv`` (fused convection) at its first step."""
         per = self.r.steps_per_launch or (j1 - j0)
         j = j0
         while j < j1:
@@ -425,6 +439,9 @@ class BatchRun:
             if j > j0:
                 self._reorder(sh)
             a = self._step_args(packed, j, c, phys_skip if j == j0 else 0, 0, noise, noise_row=j - j0)
+            if conv is not None and j == j0:
+                a.conv_column, a.conv_step, a.conv_nz = conv["conv_column"], 0, conv["conv_nz"]
+                a.conv_uniforms, a.conv_moved = conv["conv_uniforms"], conv["conv_moved"]
             _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
             self.keys_valid = self.work_key is not None
             j += c
@@ -484,7 +501,9 @@ class BatchRun:
         n = j1 - j0
         with torch.cuda.stream(main):
             self._reorder(sh)
-            if r.emanuel is not None:
+            if r.emanuel is not None and r.fuse_convection:
+                self._launch_range(packed, j0, j1, 0, noise, sh, conv=self._fused_convection(wf, j0, scratch))
+            elif r.emanuel is not None:
                 a = self._step_args(packed, j0, 1, 0, 1, noise)
                 _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
                 self.keys_valid = self.work_key is not None
@@ -693,6 +712,7 @@ class BatchRunner:
         self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
         self.reorder = True  # group particles by work class each window (results do not depend on it)
         self.steps_per_launch: int | None = None  # split each window into launches of this many steps
+        self.fuse_convection = True  # convection inside the step kernel (else its own kernel between two steps)
         self._step_stream = None
         self._slots: list[PackedWindow | None] = [None, None]
 

@@ -146,7 +146,7 @@ typedef struct glide_step_args {
     /* launch variant of the step kernel, 0 .. glide_step_launch_variants()-1: block size and
      * resident blocks per SM (0 = 128 threads x 6 blocks). The last variant is the general
      * kernel at shape 0, which every launch that sets surface_layer_override, injected noise
-     * or active_mask runs whatever this field says. Results do not depend on it. */
+     * or uniforms, or active_mask runs whatever this field says. Results do not depend on it. */
     int32_t launch_variant;
     /* optional thread -> particle permutation, device [n] (NULL = identity): thread t steps
      * particle order[t]. Results do not depend on it (state and noise are keyed by particle
@@ -158,6 +158,13 @@ typedef struct glide_step_args {
      * step (GLIDE_WORK_*): done (escaped or past the simulation length), pending (alive but
      * not yet released), or the class of the branches and substep count it took. */
     uint8_t* work_key;
+    /* optional convection fused into the launch: at step conv_step of the launch, after its
+     * physics and before its post-step, the particles active at that step are redistributed
+     * against the column in conv_column (the scratch of glide_convect with n = 0: conv_nz
+     * levels) exactly as glide_convect_redistribute does. NULL = no convection. */
+    const void* conv_column; int32_t conv_step; int32_t conv_nz;
+    const float* conv_uniforms;   /* injected uniforms [2][n], or NULL: Philox keyed by seed */
+    int32_t* conv_moved;          /* device counter of moved particles (added to), may be NULL */
 } glide_step_args;
 
 /* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */

@@ -20,7 +20,8 @@ def grid_of(run: GoldenRun) -> GridInfo:
 
 def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool = True, met_dtype: str = "f32",
                seed: int = 1234, hanna_kw: dict | None = None, launch_variant: int = 0,
-               reorder: bool = True, steps_per_launch: int | None = None) -> BatchRunner:
+               reorder: bool = True, steps_per_launch: int | None = None,
+               fuse_convection: bool = True) -> BatchRunner:
     z = run.z
     m = run.met
     grid = grid_of(run).to_device(device)
@@ -63,6 +64,7 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
     runner.launch_variant = launch_variant
     runner.reorder = reorder
     runner.steps_per_launch = steps_per_launch
+    runner.fuse_convection = fuse_convection
     return runner
 
 

@@ -295,6 +295,27 @@ def test_ring_footprint_streamed_to_host(cuda_device):
     np.testing.assert_allclose(host, dense, rtol=1e-5, atol=1e-7)
 
 
+@pytest.mark.parametrize("injected", [True, False])
+def test_fused_convection_matches_separate_launches(cuda_device, injected):
+    """Convection inside the step kernel (at the window's first step) moves the same
+    particles to the same heights as the separate redistribution kernel between a
+    one-step launch and the rest of the window."""
+    run = load_run("run_small")
+    a = run_gpu(run, cuda_device, injected=injected, fuse_convection=True)
+    b = run_gpu(run, cuda_device, injected=injected, fuse_convection=False)
+    pa, sa, aa, fa = as_numpy(a)
+    pb, sb, ab, fb = as_numpy(b)
+    np.testing.assert_array_equal(pa, pb)
+    for k in sa:
+        np.testing.assert_array_equal(sa[k], sb[k])
+    np.testing.assert_array_equal(aa, ab)
+    np.testing.assert_array_equal(a.escaped_per_step, b.escaped_per_step)
+    moved_a = [int(m.item()) for _, m in a.convection]
+    moved_b = [int(m.item()) for _, m in b.convection]
+    assert moved_a == moved_b and sum(moved_a) > 0
+    np.testing.assert_allclose(fa, fb, rtol=1e-5, atol=1e-9)
+
+
 def test_launch_variants_give_the_same_results(cuda_device):
     """Every launch variant computes the same particles (the footprint may differ in
     atomic summation order only): the fast kernels at every shape against the general
