@@ -18,6 +18,7 @@ GLIDE_OK = 0
 GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
 GLIDE_STATUS_NONFINITE_STATE, GLIDE_STATUS_BAD_ORDER = 1, 2
 GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 63, 64
+GLIDE_STEP_BATCH_MAX = 32
 
 vp = C.c_void_p
 
@@ -90,6 +91,7 @@ SIGNATURES = {
                                               C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "glide_window_pack": (C.c_int32, [C.POINTER(WindowDesc), vp]),
     "glide_step": (C.c_int32, [C.POINTER(StepArgs), vp]),
+    "glide_step_batched": (C.c_int32, [C.POINTER(StepArgs), C.c_int32, vp]),
     "glide_step_launch_variants": (C.c_int32, [C.POINTER(C.c_int32)]),
     "glide_step_launch_variant_info": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "glide_reorder_scratch_bytes": (C.c_int32, [C.c_int64, C.POINTER(C.c_size_t)]),

@@ -263,10 +263,11 @@ constexpr int kNumVariants = kNumShapes + 1;
 // the kernel is smaller, which matters because it is bound by instruction
 // issue and instruction-cache misses. Arguments that need one of those paths
 // run the GENERAL = true instantiation; both compute identical results.
-template <typename T, int THREADS, int MIN_BLOCKS, bool GENERAL>
-__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev p) {
+// The whole launch body for one batch; `block` is the block's index within the batch.
+template <typename T, bool GENERAL>
+__device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
     extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
-    const int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t th = block * blockDim.x + threadIdx.x;
     bool have = th < p.n;
     bool bad_order = false;
     int64_t i = th;  // the particle this thread steps
@@ -589,6 +590,29 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev
     }
 }
 
+template <typename T, int THREADS, int MIN_BLOCKS, bool GENERAL>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) step_kernel(const StepDev p) {
+    step_body<T, GENERAL>(p, blockIdx.x);
+}
+
+// Several independent batches (own particles, schedule, met window, footprint) in
+// one launch: batch k owns blocks [block_start[k], block_start[k + 1]).
+struct StepBatch {
+    StepDev d[GLIDE_STEP_BATCH_MAX];
+    uint32_t block_start[GLIDE_STEP_BATCH_MAX + 1];
+    int count;
+};
+
+template <typename T, bool GENERAL>
+__global__ void __launch_bounds__(128, 6) step_kernel_batched(const __grid_constant__ StepBatch b) {
+    int lo = 0, hi = b.count - 1;  // the last batch starting at or before this block (skips empty ones)
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.block_start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    step_body<T, GENERAL>(b.d[lo], (int64_t)(blockIdx.x - b.block_start[lo]));
+}
+
 template <typename T, int V, bool GENERAL>
 static void launch_shape(const StepDev& d, cudaStream_t stream, size_t smem) {
     constexpr int threads = kShapes[V].threads;
@@ -616,13 +640,14 @@ static glide_status launch_step(const StepDev& d, cudaStream_t stream, int varia
 
 using namespace glide;
 
-extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
+// Argument checks of one launch (GLIDE_OK when it can run; n == 0 passes).
+static glide_status validate_step(const glide_step_args* a) {
     if (!a) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: args is NULL");
     if (a->n < 0) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n < 0");
     if (a->n_steps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps < 1");
     if (!a->sched && a->n_steps != 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: sched is NULL but n_steps = %d", a->n_steps);
-    if (a->n == 0) return GLIDE_OK;
+    if (a->n == 0) return GLIDE_OK;  // nothing else is read
     if (!a->lon || !a->lat || !a->z || !a->weight || !a->u_prime || !a->v_prime || !a->w_prime)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: a particle state pointer is NULL");
     if (!a->active_mask && !a->rel_off)
@@ -638,7 +663,8 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", a->launch_variant);
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
     if (a->conv_column && (a->conv_nz < 2 || a->conv_step < 0 || a->conv_step >= a->n_steps))
-        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: fused convection needs conv_nz >= 2 and 0 <= conv_step < n_steps");
+        return set_error(GLIDE_ERR_INVALID_ARG,
+                         "glide_step: fused convection needs conv_nz >= 2 and 0 <= conv_step < n_steps");
     if (a->conv_column && ((uintptr_t)a->conv_column & 7u))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: conv_column must be 8-byte aligned");
     if (a->footprint && (!a->fp.z_edges || a->fp.n_z < 1 || a->fp.n_x < 1 || a->fp.n_y < 1 ||
@@ -651,6 +677,10 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     if (((uintptr_t)a->wind_packed | (uintptr_t)a->surf_packed | (uintptr_t)a->support_packed) & 15u)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: packed met must be 16-byte aligned");
 
+    return GLIDE_OK;
+}
+
+static StepDev make_step_dev(const glide_step_args* a) {
     StepDev d;
     d.n = a->n;
     d.lon = a->lon; d.lat = a->lat; d.z = a->z; d.weight = a->weight; d.ps = a->pos_stride;
@@ -683,14 +713,71 @@ extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
     d.order = a->order; d.work_key = a->work_key;
     d.conv_column = static_cast<const double*>(a->conv_column); d.conv_step = a->conv_step; d.conv_nz = a->conv_nz;
     d.conv_uniforms = a->conv_uniforms; d.conv_moved = a->conv_moved;
+    return d;
+}
+
+static bool needs_general(const StepDev& d) {
+    return d.sl_override || d.noise_sub || d.noise_mea || d.active_mask || d.conv_uniforms;
+}
+
+extern "C" glide_status glide_step(const glide_step_args* a, void* stream) {
+    if (glide_status st = validate_step(a)) return st;
+    if (a->n == 0) return GLIDE_OK;
+    const StepDev d = make_step_dev(a);
     cudaStream_t s = (cudaStream_t)stream;
-    const bool general = d.sl_override || d.noise_sub || d.noise_mea || d.active_mask || d.conv_uniforms;
-    const int variant = general ? kNumShapes : a->launch_variant;
+    const int variant = needs_general(d) ? kNumShapes : a->launch_variant;
     switch (a->met_dtype) {
         case GLIDE_MET_F32: return launch_step<float>(d, s, variant);
         case GLIDE_MET_BF16: return launch_step<__nv_bfloat16>(d, s, variant);
         case GLIDE_MET_F16: return launch_step<__half>(d, s, variant);
         default: return set_error(GLIDE_ERR_UNSUPPORTED, "glide_step: unknown met_dtype %d", a->met_dtype);
+    }
+}
+
+template <typename T>
+static glide_status launch_batched(const StepBatch& b, bool general, size_t smem, uint32_t blocks, cudaStream_t s) {
+    if (general) step_kernel_batched<T, true><<<blocks, 128, smem, s>>>(b);
+    else step_kernel_batched<T, false><<<blocks, 128, smem, s>>>(b);
+    return check_launch("glide_step_batched");
+}
+
+extern "C" glide_status glide_step_batched(const glide_step_args* args, int32_t count, void* stream) {
+    if (!args || count < 0 || count > GLIDE_STEP_BATCH_MAX)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: args NULL or count %d not in [0, %d]",
+                         count, GLIDE_STEP_BATCH_MAX);
+    StepBatch b;
+    b.count = 0;
+    bool general = false;
+    int32_t dtype = -1;
+    int max_steps = 1;
+    uint64_t blocks = 0;
+    for (int k = 0; k < count; ++k) {
+        const glide_step_args* a = args + k;
+        if (glide_status st = validate_step(a)) return st;
+        if (a->n == 0) continue;
+        if (dtype >= 0 && a->met_dtype != dtype)
+            return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: batches mix met dtypes");
+        dtype = a->met_dtype;
+        const StepDev d = make_step_dev(a);
+        general = general || needs_general(d);
+        max_steps = max(max_steps, d.n_steps);
+        b.d[b.count] = d;
+        b.block_start[b.count] = (uint32_t)blocks;
+        blocks += (uint64_t)((d.n + 127) / 128);
+        ++b.count;
+    }
+    if (b.count == 0) return GLIDE_OK;
+    if (blocks > 0x7fffffffull) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: too many particles");
+    b.block_start[b.count] = (uint32_t)blocks;
+    const size_t smem = sizeof(int32_t) * 2 * (size_t)max_steps;
+    if (smem > 48 * 1024)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: n_steps %d too large", max_steps);
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (dtype) {
+        case GLIDE_MET_F32: return launch_batched<float>(b, general, smem, (uint32_t)blocks, s);
+        case GLIDE_MET_BF16: return launch_batched<__nv_bfloat16>(b, general, smem, (uint32_t)blocks, s);
+        case GLIDE_MET_F16: return launch_batched<__half>(b, general, smem, (uint32_t)blocks, s);
+        default: return set_error(GLIDE_ERR_UNSUPPORTED, "glide_step_batched: unknown met_dtype %d", dtype);
     }
 }
 

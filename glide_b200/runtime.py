@@ -326,7 +326,7 @@ class BatchRun:
                     rows_out.index_add_(0, r_idx * fp.n_time_bins + b_idx, slices.reshape(slices.shape[0], -1))
 
                 self.sink = sink
-        self.z_edges = torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32), device=dev)
+        self.z_edges = _upload(torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32)), dev)
         # windows = runs of consecutive steps with the same hour
         self.windows: list[tuple[int, int]] = window_ranges(steps)
         self.next_window = 0
@@ -406,6 +406,69 @@ class BatchRun:
             a.work_key = self.work_key.data_ptr()
         return a
 
+    def _noise(self, j0: int, j1: int):
+        """Injected normals of steps [j0, j1), checked against the extents the kernel indexes."""
+        r = self.r
+        noise = r.noise_provider(list(range(j0, j1))) if r.noise_provider is not None else None
+        if noise is not None:
+            sub, mea = noise
+            want = (j1 - j0, r.hanna.max_substeps, 3, self.state.n)
+            if tuple(sub.shape) != want or sub.dtype != torch.float32 or not sub.is_contiguous():
+                raise ValueError(f"injected substep noise must be contiguous float32 {want}, got {tuple(sub.shape)}")
+            if r.hanna.meander_enabled and (mea is None or tuple(mea.shape) != (j1 - j0, 2, self.state.n)
+                                            or mea.dtype != torch.float32 or not mea.is_contiguous()):
+                raise ValueError("injected meander noise must be contiguous float32 (steps, 2, n)")
+        return noise
+
+    def _column_for(self, j: int, stream) -> torch.Tensor:
+        """The convection column of the window at step j (its first step), from the
+        runner's ``column_cache`` (keyed by hour and float32 RK2 weight) or built here
+        with ``glide_convect`` and no particles."""
+        r = self.r
+        st = self.steps[j]
+        key = (st.hour, float(np.float32(st.alpha)))
+        cache = r.column_cache
+        if cache is not None and key in cache:
+            return cache[key]
+        nb = C.c_size_t()
+        _abi.check(_abi.lib.glide_convect_scratch_bytes(r.grid.shape[0], C.byref(nb)), "glide_convect_scratch_bytes")
+        with torch.cuda.stream(stream):
+            col = torch.zeros(nb.value // 8, dtype=torch.float64, device=r.device)
+            a = self._convect_args(r.window_provider(st.hour), j, col, n_particles=0)
+            _abi.check(_abi.lib.glide_convect(C.byref(a), stream_handle(stream)), "glide_convect")
+        if cache is not None:
+            cache[key] = col
+        return col
+
+    def next_window_args(self, stream) -> tuple:
+        """For grouped launches (``glide_step_batched``): the next window as one launch
+        with its convection fused in, from prebuilt met (``packed_provider``) and cached
+        columns; nothing is launched but a missing column build. Returns the launch's
+        arguments and the objects they point into (keep them until the launch has run).
+        The particle order is not used (identity)."""
+        r = self.r
+        if self.done:
+            raise RuntimeError("the batch has no window left")
+        if r.packed_provider is None or r.footprint.ring > 0:
+            raise ValueError("grouped launches need a packed_provider and a dense footprint")
+        k = self.next_window
+        j0, j1 = self.windows[k]
+        self.next_window += 1
+        first = self.steps[j0]
+        packed = r.packed_provider(first.hour)
+        noise = self._noise(j0, j1)
+        keep = [packed, noise]
+        a = self._step_args(packed, j0, j1 - j0, 0, 0, noise)
+        a.order, a.work_key = None, None
+        if r.emanuel is not None:
+            col = self._column_for(j0, stream)
+            with torch.cuda.stream(stream):
+                conv = self._fused_convection(first.hour, j0, col)
+            a.conv_column, a.conv_step, a.conv_nz = conv["conv_column"], 0, conv["conv_nz"]
+            a.conv_uniforms, a.conv_moved = conv["conv_uniforms"], conv["conv_moved"]
+            keep += [col, conv["keep"]]
+        return a, keep
+
     def _reorder(self, sh) -> None:
         """Rebuild the particle order from the work keys of the last launch."""
         if self.keys_valid:
@@ -414,15 +477,15 @@ class BatchRun:
                                                      sh), "glide_reorder_by_key")
             self.order_valid = True
 
-    def _fused_convection(self, wf: WindowFields, j: int, scratch: torch.Tensor) -> dict:
+    def _fused_convection(self, hour: datetime, j: int, scratch: torch.Tensor) -> dict:
         """Fields of the window's convection fused into its first launch (at its first
-        step) against the column prebuilt on the prep stream."""
+        step) against a prebuilt column."""
         r, s = self.r, self.state
         moved = torch.zeros(1, dtype=torch.int32, device=r.device)
         u = r.conv_uniform_provider(j) if r.conv_uniform_provider is not None else None
         if u is not None and (tuple(u.shape) != (2, s.n) or u.dtype != torch.float32 or not u.is_contiguous()):
             raise ValueError(f"injected convection uniforms must be contiguous float32 (2, {s.n})")
-        self.conv_log.append((wf.time_start, moved))
+        self.conv_log.append((hour, moved))
         return {"conv_column": scratch.data_ptr(), "conv_nz": r.grid.shape[0], "conv_moved": moved.data_ptr(),
                 "conv_uniforms": None if u is None else u.data_ptr(), "keep": u}
 
@@ -486,15 +549,7 @@ class BatchRun:
             self._prepare(k)
         wf, packed, scratch, ready = self.prepared.pop(k)
         main.wait_event(ready)
-        noise = r.noise_provider(list(range(j0, j1))) if r.noise_provider is not None else None
-        if noise is not None:  # the kernel indexes these buffers: check their extents first
-            sub, mea = noise
-            want = (j1 - j0, r.hanna.max_substeps, 3, self.state.n)
-            if tuple(sub.shape) != want or sub.dtype != torch.float32 or not sub.is_contiguous():
-                raise ValueError(f"injected substep noise must be contiguous float32 {want}, got {tuple(sub.shape)}")
-            if r.hanna.meander_enabled and (mea is None or tuple(mea.shape) != (j1 - j0, 2, self.state.n)
-                                            or mea.dtype != torch.float32 or not mea.is_contiguous()):
-                raise ValueError("injected meander noise must be contiguous float32 (steps, 2, n)")
+        noise = self._noise(j0, j1)
         if main is not caller:  # the caller's work so far (state, noise) comes first
             main.wait_stream(caller)
         sh = stream_handle(main)
@@ -502,7 +557,8 @@ class BatchRun:
         with torch.cuda.stream(main):
             self._reorder(sh)
             if r.emanuel is not None and r.fuse_convection:
-                self._launch_range(packed, j0, j1, 0, noise, sh, conv=self._fused_convection(wf, j0, scratch))
+                conv = self._fused_convection(wf.time_start, j0, scratch)
+                self._launch_range(packed, j0, j1, 0, noise, sh, conv=conv)
             elif r.emanuel is not None:
                 a = self._step_args(packed, j0, 1, 0, 1, noise)
                 _abi.check(_abi.lib.glide_step(C.byref(a), sh), "glide_step")
@@ -614,6 +670,16 @@ class BatchRun:
                            self.conv_log, status)
 
 
+def launch_grouped(args: list, stream) -> None:
+    """Launch ``glide_step`` argument sets (``BatchRun.next_window_args``) as grouped
+    launches of up to ``GLIDE_STEP_BATCH_MAX`` batches on ``stream``."""
+    cap = _abi.GLIDE_STEP_BATCH_MAX
+    for i in range(0, len(args), cap):
+        chunk = args[i:i + cap]
+        arr = (_abi.StepArgs * len(chunk))(*chunk)
+        _abi.check(_abi.lib.glide_step_batched(arr, len(chunk), stream_handle(stream)), "glide_step_batched")
+
+
 class HostSliceStream:
     """A ring-footprint sink (``BatchRunner(footprint_sink=...)``) that moves the
     completed time-ago slices to pinned host memory on its own copy stream, so the
@@ -713,6 +779,7 @@ class BatchRunner:
         self.reorder = True  # group particles by work class each window (results do not depend on it)
         self.steps_per_launch: int | None = None  # split each window into launches of this many steps
         self.fuse_convection = True  # convection inside the step kernel (else its own kernel between two steps)
+        self.column_cache: dict | None = None  # (hour, alpha) -> prebuilt convection column, shared by batches
         self._step_stream = None
         self._slots: list[PackedWindow | None] = [None, None]
 

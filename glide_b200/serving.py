@@ -4,15 +4,20 @@ A request is one release (site, release time, particle count, backward duration)
 The server keeps every met window of its horizon packed and resident in HBM
 (read-only, shared by all requests), admits requests while their particle state
 and footprint fit an HBM budget and a concurrency cap, and advances every
-admitted request one met window per scheduling tick on its own CUDA stream, so
-requests of different sizes and at different cursor times overlap on the
-device. A request that arrives while others run is admitted as soon as a slot
-and memory free up. Each request's noise is keyed by its own seed and its own
-particle and step numbers, so its result does not depend on what else runs.
+admitted request one met window per scheduling tick. By default (``grouped``)
+a tick packs the next window of every admitted request — requests of different
+particle counts, release times and cursor positions, each with its own met
+window, schedule and footprint — into grouped launches (``glide_step_batched``,
+up to 32 requests each) on one stream: one launch per tick fills the GPU with
+many small requests. Otherwise each request runs its own launches on a stream of
+a pool. A request that arrives while others run is admitted as soon as the
+concurrency cap and the HBM budget allow. Each request's noise is keyed by its
+own seed and its own particle and step numbers, so its result does not depend on
+what else runs.
 
 The per-request work is exactly the batch runtime's (``glide_b200.runtime``):
-one fused ``glide_step`` launch per window (two around ``glide_convect`` on the
-window's first step).
+per window one fused step launch with the window's convection inside it; the
+convection columns of the resident windows are built once and shared.
 """
 
 from __future__ import annotations
@@ -26,7 +31,7 @@ import numpy as np
 import torch
 
 from glide_b200.runtime import (BatchRun, BatchRunner, DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig,
-                                ParticleState, hour_floor)
+                                ParticleState, hour_floor, launch_grouped)
 from glide_b200.window import GridInfo, PackedWindow, WindowFields
 
 
@@ -101,6 +106,7 @@ class ServerStats:
     completed: int = 0
     ticks: int = 0
     windows_issued: int = 0
+    launches: int = 0  # step launches (grouped launches count once)
     peak_active: int = 0
     peak_bytes: int = 0
     results: list = field(default_factory=list)
@@ -119,7 +125,8 @@ class FootprintServer:
     def __init__(self, *, grid: GridInfo, met_provider, horizon_start: datetime, horizon_end: datetime,
                  hanna: HannaConfig, emanuel: EmanuelConfig | None, footprint: FootprintSpec, domain: DomainSpec,
                  hbm_budget_bytes: float = 60e9, max_active: int = 64, n_streams: int = 16, met_dtype: str = "bf16",
-                 dt_seconds: float = 30.0, device="cuda", keep_footprints: bool = False) -> None:
+                 dt_seconds: float = 30.0, device="cuda", keep_footprints: bool = False,
+                 grouped: bool = True) -> None:
         self.device = torch.device(device)
         self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
         self.hanna, self.emanuel, self.domain = hanna, emanuel, domain
@@ -136,7 +143,12 @@ class FootprintServer:
             h = h + timedelta(hours=1)
         self.resident = _Resident(self.grid, met_provider, hours, hanna, met_dtype, self.device)
         torch.cuda.synchronize(self.device)
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, n_streams))]
+        self.grouped = bool(grouped)
+        self.column_cache: dict = {}  # (hour, alpha) -> convection column, shared by all requests
+        if self.grouped:
+            self.streams = [torch.cuda.Stream(device=self.device)]
+        else:
+            self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, n_streams))]
         self.pending: deque[FootprintRequest] = deque()
         self.active: list[_Active] = []
         self.bytes_in_use = 0
@@ -162,6 +174,8 @@ class FootprintServer:
         r = BatchRunner(grid=self.grid, window_provider=provider, hanna=self.hanna, footprint=fp,
                         domain=self.domain, emanuel=self.emanuel, met_dtype=self.met_dtype, device=self.device,
                         seed=req.seed, packed_provider=lambda hour: res[hour][1])
+        r.column_cache = self.column_cache
+        r.reorder = False  # small batches: the identity order
         return r
 
     def _admit(self, req: FootprintRequest, now_s: float) -> None:
@@ -227,15 +241,36 @@ class FootprintServer:
             self._admit(self.pending.popleft(), now)
         self.stats.peak_active = max(self.stats.peak_active, len(self.active))
         self.stats.peak_bytes = max(self.stats.peak_bytes, self.bytes_in_use)
-        for a in self.active:
-            if a.issued_all:
-                continue
-            with torch.cuda.stream(a.stream):
-                a.run.step_window(a.stream)
-                self.stats.windows_issued += 1
+        if self.grouped:
+            stream = self.streams[0]
+            args, keep, ending = [], [], []
+            for a in self.active:
+                if a.issued_all:
+                    continue
+                arg, k = a.run.next_window_args(stream)
+                args.append(arg)
+                keep.append(k)
                 if a.run.done:
-                    a.issued_all = True
-                    self._collect(a)
+                    ending.append(a)
+            if args:
+                launch_grouped(args, stream)
+                self.stats.windows_issued += len(args)
+                self.stats.launches += (len(args) + 31) // 32
+            for a in ending:
+                a.issued_all = True
+                self._collect(a)
+            del keep  # the launches are queued behind everything they read
+        else:
+            for a in self.active:
+                if a.issued_all:
+                    continue
+                with torch.cuda.stream(a.stream):
+                    a.run.step_window(a.stream)
+                    self.stats.windows_issued += 1
+                    self.stats.launches += 1
+                    if a.run.done:
+                        a.issued_all = True
+                        self._collect(a)
         finished = []
         keep = []
         for a in self.active:

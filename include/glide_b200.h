@@ -231,6 +231,16 @@ glide_status glide_window_pack(const glide_window_desc* desc, void* stream);
  * escape kill (src/lpdm/main.py:1459-1477, 690-711). */
 glide_status glide_step(const glide_step_args* args, void* stream);
 
+/* Several independent glide_step launches as one grouped launch: each of the `count`
+ * argument sets is a batch with its own particles, schedule, met window, footprint and
+ * counters, computed exactly as glide_step would; blocks of 128 threads are handed out to
+ * the batches by particle count, so batches of very different sizes fill one launch. All
+ * batches use the same met_dtype; the general kernel runs for all when any batch needs it;
+ * launch_variant is ignored. At most GLIDE_STEP_BATCH_MAX batches (no counterpart in the
+ * reference: its serving unit is one batch per process). */
+#define GLIDE_STEP_BATCH_MAX 32
+glide_status glide_step_batched(const glide_step_args* args, int32_t count, void* stream);
+
 /* Number of launch variants of the step kernel and, for variant v, its block size
  * and the resident blocks per SM it is compiled for (autotuning; the last variant is
  * the general kernel, see glide_step_args.launch_variant). */

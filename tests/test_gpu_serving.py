@@ -75,3 +75,19 @@ def test_requests_overlap_and_budget_bounds_admission(met):
     res = tight.serve(reqs, realtime=False)
     assert len(res) == len(reqs)
     assert tight.stats.peak_bytes <= one or tight.stats.peak_active == 1
+
+
+def test_grouped_and_per_stream_servers_agree(met):
+    """Grouped launches (one per tick for all requests) and one stream per request give
+    the same results."""
+    syn, grid = met
+    reqs = _requests(syn)
+    g = {r.request_id: r for r in _server(syn, grid, max_active=16, grouped=True).serve(reqs, realtime=False)}
+    srv = _server(syn, grid, max_active=16, n_streams=8, grouped=False)
+    p = {r.request_id: r for r in srv.serve(reqs, realtime=False)}
+    assert set(g) == set(p) == {r.request_id for r in reqs}
+    for k in g:
+        assert g[k].escaped == p[k].escaped and g[k].active_particle_steps == p[k].active_particle_steps
+        a, b = g[k].footprint.numpy(), p[k].footprint.numpy()
+        assert np.abs(a - b).sum() <= 1e-6 * max(np.abs(a).sum(), 1e-30)
+
