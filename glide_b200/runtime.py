@@ -657,6 +657,28 @@ class BatchRun:
         _abi.check(_abi.lib.glide_convect_redistribute(C.byref(a), stream_handle(stream)), "glide_convect_redistribute")
         self.conv_log.append((wf.time_start, moved))
 
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """Record every remaining window of the batch — particle order, step launches with
+        their fused convection, per-window packing and convection columns — into one CUDA
+        graph; ``graph.replay()`` then runs the batch with no host work, and ``finish()``
+        reads the results. The met the windows need must already be on the device
+        (device-resident window provider or ``packed_provider``), the footprint dense,
+        the noise generated, and the runner not pipelined (one stream). Replaying again
+        continues from whatever the state tensors hold (new particles can be copied in)."""
+        r = self.r
+        if r.footprint.ring > 0 or r.noise_provider is not None or r.conv_uniform_provider is not None:
+            raise ValueError("capture needs a dense footprint and generated noise")
+        if self.pipelined:
+            raise ValueError("capture needs BatchRunner(pipeline=False)")
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=r.device)
+        s.wait_stream(torch.cuda.current_stream(r.device))
+        with torch.cuda.graph(g, stream=s):
+            while self.step_window(s):
+                pass
+        torch.cuda.current_stream(r.device).wait_stream(s)
+        return g
+
     def run(self, stream=None) -> BatchOutput:
         while self.step_window(stream):
             pass
