@@ -9,8 +9,15 @@
 //   length / w* -> Hanna column turbulence at z_eval and z_eval +- 1 m (free
 //   troposphere override from the support bricks) -> well-mixed + density
 //   drift -> per-particle exact-OU substeps (clip, displacement, reflection)
-//   -> meander OU -> [post] time-ago bin, footprint residence time (cached per
-//   particle, one atomic per change of cell), escape kill.
+//   -> meander OU -> [at the window's first step, when fused] convective
+//   redistribution against the prebuilt column -> [post] time-ago bin, footprint
+//   residence time (cached per particle, one atomic per change of cell), escape
+//   kill.
+//
+// Threads map to particles through an optional permutation (the work-class
+// order) and write each particle's work class for the next order. The same body
+// runs as one batch per launch (step_kernel) or as several independent batches
+// in one grouped launch (step_kernel_batched).
 //
 // Met is read from the packed per-window bricks (window_pack.cu): the wind
 // brick holds u, v, w of both snapshots in one 32-byte (float32) or 16-byte
@@ -253,7 +260,7 @@ __device__ __forceinline__ float noise_or_philox(const StepDev& p, const float* 
 // the measured default; the others exist for the autotuner: the best shape
 // depends on the particle count (wave quantisation of a batch across 148 SMs).
 struct LaunchShape { int threads, min_blocks; };
-constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}};
+constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}, {768, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // variant kNumShapes: the general kernel at shape 0 whatever the arguments
 constexpr int kNumVariants = kNumShapes + 1;
@@ -630,6 +637,7 @@ static glide_status launch_step(const StepDev& d, cudaStream_t stream, int varia
         case 2: launch_shape<T, 2, false>(d, stream, smem); break;
         case 3: launch_shape<T, 3, false>(d, stream, smem); break;
         case 4: launch_shape<T, 4, false>(d, stream, smem); break;
+        case 5: launch_shape<T, 5, false>(d, stream, smem); break;
         case kNumShapes: launch_shape<T, 0, true>(d, stream, smem); break;
         default: return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", variant);
     }
