@@ -291,6 +291,23 @@ __device__ __forceinline__ float ou_step(float prev, float a, float drift_dt, fl
     return (a * prev + drift_dt) + amp * eta;
 }
 
+// x / c for a constant c, given r = RN(1 / c): q = RN(x r) and one correction step
+// q + RN(x - q c) r, both with fused multiply-adds (the division-by-a-known-divisor
+// scheme of P. Markstein, "IA-64 and Elementary Functions", 2000). For the divisor
+// used here (110540 m per degree of latitude) the result equals the IEEE quotient for
+// every float32 with |x| in [2^-120, 2^120] (checked over all 2^32 inputs by the
+// engine-primitive tests); zeros, tiny and huge values, infinities and NaN take the
+// IEEE division.
+__device__ __forceinline__ float div_known(float x, float c, float r) {
+    const float ax = fabsf(x);
+    if (ax >= 0x1p-120f && ax <= 0x1p120f) {
+        const float q = __fmul_rn(x, r);
+        return __fmaf_rn(__fmaf_rn(-q, c, x), r, q);
+    }
+    return x / c;
+}
+constexpr float INV_M_PER_DEG_LAT = (float)(1.0 / 110540.0);
+
 // metres per degree of longitude at a latitude (cos clamped at 0.05)
 __device__ __forceinline__ float m_per_deg_lon(float lat) { return M_PER_DEG_LON * fmaxf(fabsf(cosf(lat * DEG2RAD)), 0.05f); }
 
@@ -300,7 +317,7 @@ __device__ __forceinline__ float displace_lon(float lon, float u, float dt, floa
     return lon + ((dir * u) * dt) / m_lon;
 }
 __device__ __forceinline__ float displace_lat(float lat, float v, float dt, float dir) {
-    return lat + ((dir * v) * dt) / M_PER_DEG_LAT;
+    return lat + div_known((dir * v) * dt, M_PER_DEG_LAT, INV_M_PER_DEG_LAT);
 }
 
 // smooth-wall reflection at z_surface: (z, w) -> (2 z_surface - z, -w) below it

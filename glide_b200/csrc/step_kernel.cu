@@ -346,7 +346,8 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
                         const float u = acc[0] * om + acc[3] * alpha;
                         const float vv = acc[1] * om + acc[4] * alpha;
                         const float w = acc[2] * om + acc[5] * alpha;
-                        const float vx = u / m_per_deg_lon(qy), vy = vv / M_PER_DEG_LAT;
+                        const float vx = u / m_per_deg_lon(qy);
+                        const float vy = div_known(vv, M_PER_DEG_LAT, INV_M_PER_DEG_LAT);
                         if (stage == 0) {
                             qx = lon - hd * vx;
                             qy = lat - hd * vy;

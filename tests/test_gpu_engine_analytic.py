@@ -261,3 +261,24 @@ def test_diffusion_limit_rejects_wrong_near_surface_k(diffusion):
         got = diffusion[t_check]["particles"]
         assert np.abs(got - diffusion[t_check]["half"]).sum() > min_half, t_check
         assert np.abs(got - diffusion[t_check]["quarter"]).sum() > min_quarter, t_check
+
+
+def test_latitude_displacement_division_is_exact_for_every_float(cuda_device):
+    """The latitude displacement divides by 110540 m per degree through a reciprocal
+    and one fused correction step; over all 2^32 float32 inputs its quotient equals
+    the IEEE division (torch's elementwise tensor division) bit for bit (NaN as NaN)."""
+    eng = _engine(cuda_device, 0)
+    chunk = 1 << 27
+    c = None
+    for start in range(0, 1 << 32, chunk):
+        bits = torch.arange(start, start + chunk, dtype=torch.int64, device=cuda_device)
+        x = bits.to(torch.int32).view(torch.float32)  # every bit pattern once
+        p = torch.zeros((chunk, 4), device=cuda_device)
+        zero = torch.zeros(chunk, device=cuda_device)
+        got = eng.apply_horizontal_turbulence(p, zero, x, 1.0, backward=False)[:, 1]
+        if c is None:
+            c = torch.full((chunk,), 110540.0, device=cuda_device)
+        want = 0.0 + x / c
+        same = (got.view(torch.int32) == want.view(torch.int32)) | (torch.isnan(got) & torch.isnan(want))
+        assert bool(same.all()), (start, int((~same).sum()))
+        del bits, x, p, got, want, same
