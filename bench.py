@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
     ap.add_argument("--workload", default="single-site",
-                    choices=["single-site", "multisite", "serving", "precision"],
+                    choices=["single-site", "multisite", "serving", "precision", "regrid"],
                     help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints; "
                          "serving: Poisson stream of footprint requests through FootprintServer")
     ap.add_argument("--requests", type=int, default=2000)
@@ -404,6 +404,71 @@ def run_multisite(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_regrid(args) -> None:
+    """One met hour regridded from 37 pressure levels onto 60 AGL levels over the
+    EUROPE box (281 x 401), 9 channels with slope-corrected w and the per-level
+    pressure: ``glide_agl_regrid`` with the inputs in HBM (CUDA events, median of
+    ``--steps``), beside the reference's own ``lpdm.vertical_grid`` functions on the
+    host as ``MetReader._resample_hour_to_agl`` calls them (from the installed
+    reference in baseline/_ref, when present)."""
+    import torch
+
+    from glide_b200.regrid import regrid_hour_to_agl
+    from glide_b200.synthetic import stretched_agl_levels
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(20261209)
+    zp, ny, nx, nc = 37, 281, 401, 9
+    names = ["u", "v", "w", "t", "q", "blh", "sp", "ustar", "shf"]
+    lat, lon = np.linspace(10.0, 80.0, ny), np.linspace(-60.0, 40.0, nx)
+    terrain = np.clip(rng.normal(400.0, 400.0, (ny, nx)), 0.0, 3000.0)
+    msl = np.sort(np.concatenate([[100.0], rng.uniform(200.0, 20000.0, zp - 1)]))[::-1]  # top-of-atmosphere first
+    h_agl = (msl[:, None, None] + rng.normal(0.0, 20.0, (zp, ny, nx)) - terrain[None]).astype(np.float32)
+    fields = rng.normal(0.0, 5.0, (nc, zp, ny, nx)).astype(np.float32)
+    p_hpa = 1013.25 * np.exp(-(h_agl.astype(np.float64) + terrain[None]) / 8000.0)
+    z_sfc = (terrain * 9.80665).astype(np.float32)
+    agl = stretched_agl_levels(60, 20000.0, 10.0)
+    f_dev = torch.from_numpy(fields).to(dev)
+    h_dev = torch.from_numpy(h_agl).to(dev)
+    p_dev = torch.from_numpy(p_hpa).to(dev)
+    kw = dict(z_sfc=z_sfc, lat=lat, lon=lon, pressure_p_hpa=p_dev, device=dev)
+    for _ in range(max(args.warmup, 1)):
+        regrid_hour_to_agl(f_dev, h_dev, agl, names, **kw)
+    times = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        regrid_hour_to_agl(f_dev, h_dev, agl, names, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    gpu_s = float(np.median(times))
+    line = {"metric": "regrid s per met hour", "value": gpu_s, "unit": "s", "higher_is_better": False,
+            "workload": "regrid", "shape": {"channels": nc, "pressure_levels": zp, "agl_levels": int(agl.size),
+                                            "ny": ny, "nx": nx},
+            "note": "device time incl. the host terrain gradient and the pressure-level readback"}
+    ref = ROOT / "baseline" / "_ref"
+    if ref.is_dir():
+        sys.path.insert(0, str(ref))
+        try:
+            from lpdm.vertical_grid import (apply_agl_regrid, compute_agl_regrid_weights, slope_correct_w,
+                                            terrain_gradient)
+
+            t = time.perf_counter()
+            w = compute_agl_regrid_weights(h_agl, agl)
+            arr = apply_agl_regrid(fields, w)
+            dhdx, dhdy = terrain_gradient(z_sfc / 9.80665, lat, lon)
+            arr[2] = slope_correct_w(arr[2], arr[0], arr[1], dhdx, dhdy, agl, float(agl[-1]))
+            apply_agl_regrid(np.ascontiguousarray(p_hpa)[None], w)[0].mean(axis=(1, 2))
+            cpu_s = time.perf_counter() - t
+            line["reference_cpu"] = {"value": cpu_s, "unit": "s", "cores": torch.get_num_threads(),
+                                     "kind": "reference", "sample": "the same hour through lpdm.vertical_grid"}
+        except Exception as exc:  # the reference install is optional here
+            line["reference_cpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+    print(json.dumps(line), flush=True)
+
+
 def run_serving(args) -> None:
     """Poisson stream (default 5 requests/s, 2,000 requests) of footprint requests:
     site among 56, release time uniform in 48 h, particles log-uniform in
@@ -692,6 +757,9 @@ def main() -> None:
         return
     if args.impl == "reference-gpu":
         run_reference_gpu(args)
+        return
+    if args.workload == "regrid":
+        run_regrid(args)
         return
     if args.workload == "multisite":
         run_multisite(args)

@@ -19,6 +19,7 @@ GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
 GLIDE_STATUS_NONFINITE_STATE, GLIDE_STATUS_BAD_ORDER = 1, 2
 GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 63, 64
 GLIDE_STEP_BATCH_MAX = 32
+GLIDE_REGRID_MAX_LEVELS = 256
 
 vp = C.c_void_p
 
@@ -80,7 +81,15 @@ class OuArgs(C.Structure):
                 ("drift_scalar", C.c_float), ("noise", vp), ("seed", C.c_uint64), ("counter", C.c_uint32)]
 
 
-STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs)
+class RegridArgs(C.Structure):
+    _fields_ = [("n_channels", C.c_int32), ("zp", C.c_int32), ("za", C.c_int32), ("ny", C.c_int32),
+                ("nx", C.c_int32), ("height_agl_p", vp), ("agl_levels", vp), ("fields_p", vp), ("fields_agl", vp),
+                ("pressure_p_hpa", vp), ("pressure_level_hpa", vp), ("u_channel", C.c_int32),
+                ("v_channel", C.c_int32), ("w_channel", C.c_int32), ("dhdx", vp), ("dhdy", vp),
+                ("slope_f32", C.c_int32), ("z_top_m", C.c_double), ("scratch", vp), ("scratch_bytes", C.c_size_t)]
+
+
+STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs, RegridArgs)
 
 # every exported symbol with (restype, argtypes)
 SIGNATURES = {
@@ -101,6 +110,8 @@ SIGNATURES = {
     "glide_displace_horizontal": (C.c_int32, [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_float, C.c_int32, vp]),
     "glide_reflect_surface": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, C.c_float, vp]),
     "glide_rk2_stage": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, C.c_int64, C.c_float, vp, C.c_int64, vp]),
+    "glide_agl_regrid_scratch_bytes": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
+    "glide_agl_regrid": (C.c_int32, [C.POINTER(RegridArgs), vp]),
     "glide_footprint_accumulate": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_float,
                                                C.POINTER(FootprintGrid), vp, vp]),
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),

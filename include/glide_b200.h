@@ -200,6 +200,27 @@ typedef struct glide_ou_args {
     uint64_t seed; uint32_t counter;
 } glide_ou_args;
 
+/* Pressure-level -> terrain-following (AGL) regrid of one met hour
+ * (MetReader._resample_hour_to_agl, src/lpdm/met_reader.py:641-693, with
+ * lpdm/vertical_grid.py:166-318). Device arrays unless noted. */
+#define GLIDE_REGRID_MAX_LEVELS 256
+typedef struct glide_regrid_args {
+    int32_t n_channels, zp, za, ny, nx;
+    const float* height_agl_p;     /* [zp][ny][nx] AGL height of each stored level (may be negative) */
+    const double* agl_levels;      /* HOST [za], strictly ascending target heights */
+    const float* fields_p;         /* [n_channels][zp][ny][nx] */
+    float* fields_agl;             /* [n_channels][za][ny][nx] output */
+    const double* pressure_p_hpa;  /* [zp][ny][nx], or NULL */
+    double* pressure_level_hpa;    /* [za] output: bbox mean of the regridded pressure */
+    int32_t u_channel, v_channel, w_channel; /* w_channel < 0: no slope correction of w */
+    const double* dhdx; const double* dhdy;  /* [ny][nx] terrain slopes, m/m (terrain_gradient) */
+    int32_t slope_f32;             /* bit 0 / 1: dhdx / dhdy hold float32 values, multiplied in float32
+                                    * as numpy multiplies two float32 arrays (the reference's dhdy is
+                                    * float32 when the terrain is) */
+    double z_top_m;                /* top of the taper of the slope correction */
+    void* scratch; size_t scratch_bytes;     /* glide_agl_regrid_scratch_bytes(za, ny, nx) */
+} glide_regrid_args;
+
 /* --- library ------------------------------------------------------------------ */
 
 /* Version of this ABI (major * 10000 + minor * 100 + patch). */
@@ -210,7 +231,8 @@ glide_status glide_last_error(char* buf, size_t len);
 
 /* sizeof of the ABI structs, in declaration order: glide_grid, glide_window_desc,
  * glide_step_sched, glide_footprint_grid, glide_step_args, glide_convect_args,
- * glide_ou_args. Lets a binding verify its struct layouts. Writes min(n, 7) values. */
+ * glide_ou_args, glide_regrid_args. Lets a binding verify its struct layouts.
+ * Writes min(n, 8) values. */
 glide_status glide_abi_struct_sizes(size_t* out, int32_t n);
 
 /* --- per-window met packing ------------------------------------------------------
@@ -279,6 +301,14 @@ glide_status glide_reflect_surface(int64_t n, float* z, int64_t z_stride, float*
 /* out[i][0..3) = x[i][0..3) - h * v[i][0..3) (strides >= 3, in floats) */
 glide_status glide_rk2_stage(int64_t n, const float* x, int64_t x_stride, const float* v, int64_t v_stride, float h,
                              float* out, int64_t out_stride, void* stream);
+
+/* --- met regrid ------------------------------------------------------------------
+ * compute_agl_regrid_weights + apply_agl_regrid + slope_correct_w + the per-level
+ * bbox-mean pressure of MetReader._resample_hour_to_agl (src/lpdm/met_reader.py:
+ * 641-693; src/lpdm/vertical_grid.py:166-258, 296-318) for one hour: weights in
+ * FP64, channels interpolated as torch.lerp does, the slope correction in FP64. */
+glide_status glide_agl_regrid_scratch_bytes(int32_t za, int32_t ny, int32_t nx, size_t* bytes);
+glide_status glide_agl_regrid(const glide_regrid_args* args, void* stream);
 
 /* --- footprint accumulation alone -----------------------------------------------
  * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the

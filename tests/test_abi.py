@@ -60,6 +60,14 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert _abi.lib.glide_window_packed_bytes(60, 281, 401, 0, C.byref(wb), C.byref(sb), C.byref(pb)) == 0
     assert wb.value == 60 * 281 * 401 * 32 and sb.value == 281 * 401 * 64
     assert _abi.lib.glide_window_packed_bytes(60, 281, 401, 7, C.byref(wb), C.byref(sb), C.byref(pb)) == 3
+    r = _abi.RegridArgs()
+    assert _abi.lib.glide_agl_regrid(C.byref(r), None) == 1 and "sizes" in _abi.last_error()
+    levels = (C.c_double * 3)(0.0, 50.0, 20.0)  # not ascending
+    r.n_channels, r.zp, r.za, r.ny, r.nx = 1, 4, 3, 2, 2
+    r.height_agl_p = r.fields_p = r.fields_agl = r.scratch = 64
+    r.agl_levels = C.cast(levels, C.c_void_p)
+    assert _abi.lib.glide_agl_regrid(C.byref(r), None) == 1 and "ascending" in _abi.last_error()
+    assert _abi.lib.glide_agl_regrid_scratch_bytes(3, 2, 2, C.byref(nb)) == 0 and nb.value == 3 * 4 * 12 + 32
 
 
 def test_check_raises_with_text():
