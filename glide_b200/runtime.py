@@ -535,9 +535,17 @@ class BatchRun:
         self.prepared[k] = (wf, packed, scratch, ev)
 
     def step_window(self, stream=None) -> bool:
-        """Issue the launches of the next met window; False when the batch is done."""
+        """Issue the launches of the next met window; False when the batch is done.
+        Each window is an NVTX range named after its hour (for NVIDIA's profilers)."""
         if self.done:
             return False
+        torch.cuda.nvtx.range_push(f"glide window {self.steps[self.windows[self.next_window][0]].hour:%Y-%m-%dT%H}")
+        try:
+            return self._step_window(stream)
+        finally:
+            torch.cuda.nvtx.range_pop()
+
+    def _step_window(self, stream) -> bool:
         r = self.r
         k = self.next_window
         j0, j1 = self.windows[k]
