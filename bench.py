@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
+    ap.add_argument("--dense-footprints", action="store_true",
+                    help="multisite: move completed slices to the host dense (default: as (cell, value) lists)")
     return ap.parse_args()
 
 
@@ -350,7 +352,8 @@ def multisite_workload(args, rank: int = 0):
 
 def run_multisite(args) -> None:
     """The batched multi-release job: every release in one particle batch, one fused
-    launch per met window, completed time_ago slices streamed to pinned host memory."""
+    launch per met window, completed time_ago slices streamed to pinned host memory
+    (compacted to (cell, value) lists on the device unless --dense-footprints)."""
     import torch
 
     from glide_b200.runtime import BatchRunner, ParticleState
@@ -363,17 +366,36 @@ def run_multisite(args) -> None:
     syn = SyntheticMet(cfg["spec"], device=dev)
     grid = grid_from_synthetic(syn).to_device(dev)
     from glide_b200.runtime import HostSliceStream
+    from glide_b200.sparse import SparseSliceStream
 
     stream = torch.cuda.current_stream()
     fp = cfg["footprint"]
     totals = torch.zeros(fp.n_releases, fp.n_time_bins, dtype=torch.float64, device=dev)
-    # completed slices go to pinned host memory on a copy stream (a writer would take them from on_host)
-    to_host = HostSliceStream(dev, (len(fp.z_edges) - 1, fp.n_y, fp.n_x), capacity=fp.n_releases)
+    slice_shape = (len(fp.z_edges) - 1, fp.n_y, fp.n_x)
+    host_total = [0.0]
+    # completed slices go to pinned host memory on a copy stream (a writer would take them from on_host):
+    # as (cell, value) lists compacted on the device, or dense
+    if args.dense_footprints:
+        to_host = HostSliceStream(dev, slice_shape, capacity=fp.n_releases)
 
-    def sink(r_idx, b_idx, slices):
-        k = slices.shape[0]
-        totals.view(-1).index_add_(0, r_idx * fp.n_time_bins + b_idx, slices.view(k, -1).sum(dim=1, dtype=torch.float64))
-        to_host(r_idx, b_idx, slices)
+        def sink(r_idx, b_idx, slices):
+            k = slices.shape[0]
+            totals.view(-1).index_add_(0, r_idx * fp.n_time_bins + b_idx,
+                                       slices.view(k, -1).sum(dim=1, dtype=torch.float64))
+            to_host(r_idx, b_idx, slices)
+    else:
+        def on_host(r_idx, b_idx, off, cell, value):
+            host_total[0] += float(value.sum(dtype=np.float64))  # the host's view of what arrived
+
+        to_host = SparseSliceStream(dev, slice_shape, on_host=on_host, capacity=fp.n_releases)
+
+        class SparseSink:
+            def from_rows(self, rows, flat, r_idx, b_idx):
+                totals.view(-1).index_add_(0, r_idx * fp.n_time_bins + b_idx,
+                                           rows.index_select(0, flat).sum(dim=1, dtype=torch.float64))
+                to_host.from_rows(rows, flat, r_idx, b_idx)
+
+        sink = SparseSink()
 
     runner = BatchRunner(grid=grid, window_provider=lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid),
                          hanna=cfg["hanna"], footprint=fp, domain=cfg["domain"], emanuel=cfg["emanuel"],
@@ -402,8 +424,12 @@ def run_multisite(args) -> None:
             "releases": cfg["n_releases"], "particles": n_total, "outer_steps": len(run.steps),
             "windows": len(run.windows), "active_particle_steps": active_ps,
             "buffer_particle_steps_per_s": n_total * len(run.steps) / t, "device_s": t, "wall_s": wall,
-            "dtype": args.met, "footprint_d2h_bytes": to_host.bytes_moved, "status": int(run.status.item()),
+            "dtype": args.met, "footprint_form": "dense" if args.dense_footprints else "sparse",
+            "footprint_d2h_bytes": to_host.bytes_moved, "status": int(run.status.item()),
             "footprint_total": float(totals.sum().item()), "clocks": clocks.summary()}
+    if not args.dense_footprints:
+        line.update({"footprint_dense_bytes": to_host.dense_bytes, "footprint_entries": to_host.entries,
+                     "footprint_total_host": host_total[0], "short_copies": to_host.short_copies})
     print(json.dumps(line), flush=True)
 
 

@@ -17,6 +17,7 @@ LIB_PATH = Path(os.environ.get("GLIDE_B200_LIBRARY") or Path(__file__).resolve()
 GLIDE_OK = 0
 GLIDE_MET_F32, GLIDE_MET_BF16, GLIDE_MET_F16 = 0, 1, 2
 GLIDE_STATUS_NONFINITE_STATE, GLIDE_STATUS_BAD_ORDER = 1, 2
+GLIDE_STATUS_BAD_ROW, GLIDE_STATUS_COMPACT_OVERFLOW = 4, 8
 GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 63, 64
 GLIDE_STEP_BATCH_MAX = 32
 GLIDE_REGRID_MAX_LEVELS = 256
@@ -89,7 +90,13 @@ class RegridArgs(C.Structure):
                 ("slope_f32", C.c_int32), ("z_top_m", C.c_double), ("scratch", vp), ("scratch_bytes", C.c_size_t)]
 
 
-STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs, RegridArgs)
+class CompactArgs(C.Structure):
+    _fields_ = [("rows", vp), ("n_rows", C.c_int64), ("cells", C.c_int64), ("row_index", vp), ("k", C.c_int32),
+                ("clear", C.c_int32), ("slice_offset", vp), ("out_cell", vp), ("out_value", vp),
+                ("capacity", C.c_int64), ("status", vp), ("scratch", vp), ("scratch_bytes", C.c_size_t)]
+
+
+STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs, RegridArgs, CompactArgs)
 
 # every exported symbol with (restype, argtypes)
 SIGNATURES = {
@@ -112,6 +119,8 @@ SIGNATURES = {
     "glide_rk2_stage": (C.c_int32, [C.c_int64, vp, C.c_int64, vp, C.c_int64, C.c_float, vp, C.c_int64, vp]),
     "glide_agl_regrid_scratch_bytes": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_size_t)]),
     "glide_agl_regrid": (C.c_int32, [C.POINTER(RegridArgs), vp]),
+    "glide_footprint_compact_scratch_bytes": (C.c_int32, [C.c_int32, C.c_int64, C.POINTER(C.c_size_t)]),
+    "glide_footprint_compact": (C.c_int32, [C.POINTER(CompactArgs), vp]),
     "glide_footprint_accumulate": (C.c_int32, [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_float,
                                                C.POINTER(FootprintGrid), vp, vp]),
     "glide_convect_scratch_bytes": (C.c_int32, [C.c_int32, C.POINTER(C.c_size_t)]),

@@ -26,7 +26,7 @@ LIB_NAME = "libglide_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
 SOURCES = ("abi.cu", "window_pack.cu", "step_kernel.cu", "footprint.cu", "convection.cu", "reorder.cu",
-           "primitives.cu", "regrid.cu")
+           "primitives.cu", "regrid.cu", "compact.cu")
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr"]

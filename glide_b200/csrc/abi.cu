@@ -40,9 +40,9 @@ extern "C" glide_status glide_last_error(char* buf, size_t len) {
 
 extern "C" glide_status glide_abi_struct_sizes(size_t* out, int32_t n) {
     if (!out || n < 0) return GLIDE_ERR_INVALID_ARG;
-    const size_t sizes[8] = {sizeof(glide_grid), sizeof(glide_window_desc), sizeof(glide_step_sched),
+    const size_t sizes[9] = {sizeof(glide_grid),        sizeof(glide_window_desc), sizeof(glide_step_sched),
                              sizeof(glide_footprint_grid), sizeof(glide_step_args), sizeof(glide_convect_args),
-                             sizeof(glide_ou_args), sizeof(glide_regrid_args)};
-    for (int i = 0; i < n && i < 8; ++i) out[i] = sizes[i];
+                             sizeof(glide_ou_args),     sizeof(glide_regrid_args), sizeof(glide_compact_args)};
+    for (int i = 0; i < n && i < 9; ++i) out[i] = sizes[i];
     return GLIDE_OK;
 }

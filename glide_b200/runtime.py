@@ -623,6 +623,13 @@ class BatchRun:
         # without waiting for the device (a scalar index_put_ through advanced indexing does not)
         rows = self.footprint.view(fp.n_releases * fp.ring, -1)
         flat = ri * fp.ring + bi % fp.ring
+        from_rows = getattr(self.sink, "from_rows", None)
+        if from_rows is not None:  # the sink reads the slices from the ring and clears their slots
+            flat_host = idx[0] * fp.ring + idx[1] % fp.ring
+            if np.unique(flat_host).size != flat_host.size:
+                raise RuntimeError("ring flush names a ring slot twice")
+            from_rows(rows, flat, ri, bi)
+            return
         slices = rows.index_select(0, flat).view((-1,) + tuple(self.footprint.shape[2:]))
         self.sink(ri, bi, slices)
         rows.index_fill_(0, flat, 0.0)

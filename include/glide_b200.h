@@ -35,6 +35,8 @@ enum { GLIDE_MET_F32 = 0, GLIDE_MET_BF16 = 1, GLIDE_MET_F16 = 2 };
 enum {
     GLIDE_STATUS_NONFINITE_STATE = 1u << 0, /* a particle's state became NaN/inf */
     GLIDE_STATUS_BAD_ORDER = 1u << 1,       /* glide_step_args.order held an index outside [0, n) */
+    GLIDE_STATUS_BAD_ROW = 1u << 2,         /* glide_compact_args.row_index held a row outside [0, n_rows) */
+    GLIDE_STATUS_COMPACT_OVERFLOW = 1u << 3, /* glide_footprint_compact: more entries than capacity */
 };
 
 /* work classes written to glide_step_args.work_key: GLIDE_WORK_DONE, GLIDE_WORK_PENDING, or
@@ -221,6 +223,24 @@ typedef struct glide_regrid_args {
     void* scratch; size_t scratch_bytes;     /* glide_agl_regrid_scratch_bytes(za, ny, nx) */
 } glide_regrid_args;
 
+/* Sparse form of completed footprint slices (glide_footprint_compact). A slice is one
+ * (release, time_ago) block [n_z][n_y][n_x] of the footprint, stored as one row of
+ * `cells` float32. Device memory throughout. */
+typedef struct glide_compact_args {
+    float* rows;                   /* [n_rows][cells] slices; cleared entries are set to 0 */
+    int64_t n_rows;
+    int64_t cells;                 /* values per slice, 1 .. INT32_MAX */
+    const int64_t* row_index;      /* [k] rows to compact, in output order */
+    int32_t k;
+    int32_t clear;                 /* != 0: set every compacted row to 0 (the rows must be distinct) */
+    int64_t* slice_offset;         /* [k + 1] out: slice s holds entries [slice_offset[s], slice_offset[s+1]) */
+    int32_t* out_cell;             /* [capacity] out: cell index within the slice, ascending per slice */
+    float* out_value;              /* [capacity] out: the value, bit-unchanged */
+    int64_t capacity;
+    uint32_t* status;              /* device status word (GLIDE_STATUS_*), may be NULL */
+    void* scratch; size_t scratch_bytes;  /* glide_footprint_compact_scratch_bytes(k, cells) */
+} glide_compact_args;
+
 /* --- library ------------------------------------------------------------------ */
 
 /* Version of this ABI (major * 10000 + minor * 100 + patch). */
@@ -231,8 +251,8 @@ glide_status glide_last_error(char* buf, size_t len);
 
 /* sizeof of the ABI structs, in declaration order: glide_grid, glide_window_desc,
  * glide_step_sched, glide_footprint_grid, glide_step_args, glide_convect_args,
- * glide_ou_args, glide_regrid_args. Lets a binding verify its struct layouts.
- * Writes min(n, 8) values. */
+ * glide_ou_args, glide_regrid_args, glide_compact_args. Lets a binding verify its
+ * struct layouts. Writes min(n, 9) values. */
 glide_status glide_abi_struct_sizes(size_t* out, int32_t n);
 
 /* --- per-window met packing ------------------------------------------------------
@@ -319,6 +339,21 @@ glide_status glide_footprint_accumulate(int64_t n, const float* lon, const float
                                         int64_t weight_stride, const int32_t* t_idx,
                                         const int32_t* release_idx, float dt_seconds,
                                         const glide_footprint_grid* grid, float* footprint, void* stream);
+
+/* --- sparse footprint slices -----------------------------------------------------
+ * The device half of streaming completed footprint slices to the output writer
+ * (OutputWriter.write_footprint_region, src/lpdm/output_writer.py:215-243, which takes
+ * dense (release, T, Z, Y, X) blocks): most cells of a slice are zero, so the slices
+ * leave the device as (cell, value) lists. Entry e of the output is a cell whose float32
+ * bit pattern is not zero (so -0.0 and NaN are kept and a dense slice is rebuilt
+ * bit-exactly by writing the values into zeros); slices in row_index order, cells
+ * ascending within a slice. A row outside [0, n_rows) sets GLIDE_STATUS_BAD_ROW and
+ * yields an empty slice. slice_offset is always written; when its last entry (the total)
+ * exceeds capacity, GLIDE_STATUS_COMPACT_OVERFLOW is set and nothing else is written or
+ * cleared. Three launches on `stream`, no synchronisation. No counterpart in the
+ * reference, which copies the dense footprint to the host. */
+glide_status glide_footprint_compact_scratch_bytes(int32_t k, int64_t cells, size_t* bytes);
+glide_status glide_footprint_compact(const glide_compact_args* args, void* stream);
 
 /* --- Emanuel convection ------------------------------------------------------------
  * EmanuelReducedConvection.maybe_convect (src/lpdm/convection/emanuel.py:570-716)

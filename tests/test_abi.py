@@ -83,3 +83,32 @@ def test_empty_launch_is_a_no_op_without_a_device():
     c = _abi.ConvectArgs()
     c.n, c.nz, c.ny, c.nx = 0, 4, 2, 2
     assert _abi.lib.glide_convect(C.byref(c), None) == 1  # met inputs are still required
+
+
+def test_footprint_compact_arguments_are_checked_without_a_device():
+    nb = C.c_size_t()
+    lib = _abi.lib
+    assert lib.glide_footprint_compact_scratch_bytes(3, 4097, C.byref(nb)) == 0
+    assert nb.value == 8 * (3 * 3 + 1) + 4 * 3 * 3  # 3 tiles of 2048 cells per slice
+    assert lib.glide_footprint_compact_scratch_bytes(0, 1, C.byref(nb)) == 0 and nb.value == 8
+    assert lib.glide_footprint_compact_scratch_bytes(-1, 10, C.byref(nb)) == 1 and "negative" in _abi.last_error()
+    assert lib.glide_footprint_compact_scratch_bytes(1, 0, C.byref(nb)) == 1 and "cells" in _abi.last_error()
+    assert lib.glide_footprint_compact_scratch_bytes(1, 2**31, C.byref(nb)) == 1
+    assert lib.glide_footprint_compact_scratch_bytes(2**30, 2**20, C.byref(nb)) == 1 and "tiles" in _abi.last_error()
+    assert lib.glide_footprint_compact(None, None) == 1 and "NULL" in _abi.last_error()
+    a = _abi.CompactArgs()
+    a.k, a.cells, a.n_rows, a.capacity = 2, 100, 4, 200
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "NULL" in _abi.last_error()
+    a.rows = a.row_index = a.slice_offset = a.out_cell = a.out_value = 64
+    a.scratch, a.scratch_bytes = 64, 8
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "scratch" in _abi.last_error()
+    a.scratch_bytes = 1024
+    a.row_index = 68  # not 8-byte aligned
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "misaligned" in _abi.last_error()
+    a.row_index = 64
+    a.capacity = -1
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "capacity" in _abi.last_error()
+    a.capacity, a.n_rows = 200, 2**62
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "n_rows" in _abi.last_error()
+    a.n_rows, a.capacity, a.out_cell = 4, 10, None
+    assert lib.glide_footprint_compact(C.byref(a), None) == 1 and "capacity > 0" in _abi.last_error()
