@@ -159,17 +159,17 @@ class SparseSliceStream:
         total = int(off[k])
         if total > spec:  # the speculation was short: copy the rest now
             self.short_copies += 1
-            if total > slot["h"]:
+            if total > slot["h"]:  # larger host buffers, keeping the entries that have landed
+                old_cell, old_value = slot["h_cell"], slot["h_value"]
                 self._host_entries(slot, total)
-                lo = 0  # new host buffers: copy every entry
-            else:
-                lo = spec
+                slot["h_cell"][:spec].copy_(old_cell[:spec])
+                slot["h_value"][:spec].copy_(old_value[:spec])
             with torch.cuda.stream(self.copy_stream):
-                slot["h_cell"][lo:total].copy_(slot["cell"][lo:total], non_blocking=True)
-                slot["h_value"][lo:total].copy_(slot["value"][lo:total], non_blocking=True)
+                slot["h_cell"][spec:total].copy_(slot["cell"][spec:total], non_blocking=True)
+                slot["h_value"][spec:total].copy_(slot["value"][spec:total], non_blocking=True)
                 ev = self.copy_stream.record_event()
             ev.synchronize()
-            self.bytes_moved += (total - lo) * 8
+            self.bytes_moved += (total - spec) * 8
         if k > 0:
             self.per_slice = max(self.per_slice, float(np.diff(off).max()))
         self.entries += total
