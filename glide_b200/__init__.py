@@ -3,8 +3,11 @@
 Submodules: ``runtime`` (fused batch runtime), ``schemes`` (the reference's
 plug-in interface: ``hanna_1982_b200``, ``emanuel_reduced_b200``,
 ``FootprintGridderB200``), ``serving`` (continuous-batching footprint server),
-``window`` (met windows, packing, host streaming), ``autotune``, ``replicas``,
-``synthetic`` (seeded synthetic met), ``met`` (``HourlyMetTensors``). The CUDA
+``window`` (met windows, packing, host streaming), ``sparse`` (footprint slices
+compacted on the device and streamed to the host, reassembled per release for the
+region writer), ``regrid`` (pressure-level -> terrain-following met regrid),
+``engine`` (``GPUEngine`` primitives), ``autotune``, ``replicas``, ``synthetic``
+(seeded synthetic met), ``met`` (``HourlyMetTensors``). The CUDA
 library is ``libglide_b200.so`` next to this file (``python -m glide_b200.build``);
 importing a module that needs it raises ``ImportError`` when it is missing.
 """
