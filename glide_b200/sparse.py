@@ -57,7 +57,8 @@ def compact_rows(rows: torch.Tensor, row_index: torch.Tensor, *, clear: bool = F
     cap = k * cells if capacity is None else int(capacity)
     dev = rows.device
     if out is None:
-        out = (torch.empty(k + 1, dtype=torch.int64, device=dev), torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
+        out = (torch.empty(k + 1, dtype=torch.int64, device=dev),
+               torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
                torch.empty(max(cap, 1), dtype=torch.float32, device=dev))
     off, cell, value = out
     if off.numel() < k + 1 or cell.numel() < cap or value.numel() < cap:

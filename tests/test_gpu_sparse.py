@@ -124,8 +124,10 @@ def test_stream_dense_protocol(cuda_device):
     rng = np.random.default_rng(7)
     shape = (1, 37, 53)
     got = []
-    sink = SparseSliceStream(cuda_device, shape, on_host=lambda r, b, o, c, v: got.append((r, b, densify(o, c, v, shape))),
-                             buffers=2, initial_density=0.0)
+    def on_host(r, b, o, c, v):
+        got.append((r, b, densify(o, c, v, shape)))
+
+    sink = SparseSliceStream(cuda_device, shape, on_host=on_host, buffers=2, initial_density=0.0)
     calls = []
     for j in range(4):
         x = _rows(rng, 6, int(np.prod(shape))).reshape((6,) + shape)
