@@ -81,10 +81,12 @@ def footprint_indices(xyz, active, t_idx, release_idx, g: GridSpec, dt):
     return flat, valid
 
 
-def accumulate(fp_flat, xyz, active, weights, t_idx, release_idx, g: GridSpec, delta: float, dt):
-    """``FootprintGridder.accumulate``: scatter-add ``weight * valid * dt`` in particle order."""
+def accumulate(fp_flat, xyz, active, weights, t_idx, release_idx, g: GridSpec, delta: float, dt, fdt=None):
+    """``FootprintGridder.accumulate``: scatter-add ``weight * valid * dt`` in particle order;
+    the cell indices in ``dt``, the contributions formed and added in ``fdt`` (default ``dt``)."""
+    fdt = fdt or dt
     flat, valid = footprint_indices(xyz, active, t_idx, release_idx, g, dt)
-    w_eff = weights.astype(dt) * valid.astype(dt) * dt(delta)
+    w_eff = weights.astype(fdt) * valid.astype(fdt) * fdt(delta)
     np.add.at(fp_flat, flat, w_eff)
 
 
@@ -138,6 +140,18 @@ class BatchResult:
     convection: list = field(default_factory=list)  # (window start, fires, n_moved)
     n_steps: int = 0
     snapshots: dict = field(default_factory=dict)
+    # per-step diagnostics (main.py:1565-1566): mean (lon, lat, z) of all particles after the
+    # step, and the grid-mean (u, v, w) of the window lerped by the step's RK2 weight
+    diag_pos: list = field(default_factory=list)
+    diag_wind: list = field(default_factory=list)
+
+
+def wind_mean(win: dict, alpha: float) -> np.ndarray:
+    """``_advection_alpha_wind_mean``'s wind (main.py:892-938): float32 grid means of u, v, w of
+    the two snapshots, lerped as ``mean_start * (1 - alpha) + mean_end * alpha`` in float32."""
+    m = [np.array([np.mean(win[c][s], dtype=np.float64) for c in ("u", "v", "w")]).astype(np.float32)
+         for s in (0, 1)]
+    return m[0] * np.float32(1.0 - alpha) + m[1] * np.float32(alpha)
 
 
 def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win_end_off, release_idx,
@@ -148,7 +162,7 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
               dtype=np.float32, conv_dtype=None, max_steps: int | None = None,
               init_state: dict | None = None, init_alive=None, step_offset: int = 0,
               inputs_cache: dict | None = None, convect_first: bool = True,
-              snapshot_steps: tuple = ()) -> BatchResult:
+              snapshot_steps: tuple = (), fp_dtype=None) -> BatchResult:
     """The static cursor loop of ``main._run`` for one batch (main.py:1382-1477).
 
     ``init_state`` / ``init_alive`` / ``step_offset`` resume a batch mid-way: the
@@ -156,9 +170,12 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
     ``step_offset`` (the noise rows). ``inputs_cache`` keeps the per-window support
     stacks across calls; ``convect_first=False`` treats the first window as already
     convected (a resumed mid-window start). ``snapshot_steps``: step counts after
-    which the particles are recorded in ``BatchResult.snapshots``."""
+    which the particles are recorded in ``BatchResult.snapshots``. ``fp_dtype`` is the
+    footprint's value type (default: ``dtype``): float64 with float32 particles is the
+    FP64 gridder fed float32 positions and weights."""
     dt = dtype
     conv_dt = conv_dtype or dtype
+    fdt = fp_dtype or dtype
     n = particles.shape[1]
     p = particles.astype(dt).copy()
     state = {k: np.zeros(n, dtype=dt) for k in ("u_prime", "v_prime", "w_prime")}
@@ -168,7 +185,7 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
     if init_state is not None:
         state = {k: np.asarray(init_state[k], dtype=dt).copy() for k in state}
     alive = np.ones(n, dtype=bool) if init_alive is None else np.asarray(init_alive, dtype=bool).copy()
-    fp = np.zeros(int(np.prod(grid.shape)), dtype=dt)
+    fp = np.zeros(int(np.prod(grid.shape)), dtype=fdt)
     rel_off = rel_off.astype(dt)
     win_end_off = win_end_off.astype(dt)
     res = BatchResult(p, state, alive, fp.reshape(grid.shape))
@@ -202,11 +219,13 @@ def run_batch(*, get_window: Callable[[datetime], dict], particles, rel_off, win
                 res.convection.append((win["time_start"], col.fires, n_moved))
             last_bracket = win["time_start"]
         t_idx = time_ago_index(win_end_off, cur, grid.n_time_bins, dt)
-        accumulate(fp, p[:3], active, p[3], t_idx, release_idx, grid, delta, dt)
+        accumulate(fp, p[:3], active, p[3], t_idx, release_idx, grid, delta, dt, fdt)
         escaped = active & ~within_met_domain(p[:3], domain, dt)
         alive = alive & ~escaped
         res.escaped_per_step.append(int(escaped.sum()))
         res.active_per_step.append(int(active.sum()))
+        res.diag_pos.append(np.mean(p[:3].astype(np.float64), axis=1).astype(dt))
+        res.diag_wind.append(wind_mean(win, alpha))
         t_cursor = t_cursor - timedelta(seconds=delta)
         step += 1
         if step in snapshot_steps:

@@ -20,7 +20,7 @@ if str(GOLDEN) not in sys.path:
 
 from noise import conv_uniforms, noise_block, step_noise  # noqa: E402,F401
 
-from glide_b200.synthetic import SyntheticMet, SyntheticMetSpec  # noqa: E402
+from glide_b200.synthetic import SyntheticMet, SyntheticMetSpec, config_met_spec  # noqa: E402
 
 FIELDS = ("u", "v", "w", "t", "q", "blh", "sp", "ustar", "shf")
 
@@ -83,7 +83,10 @@ def load_run(name: str) -> GoldenRun:
         met = MetArrays({n: z[f"met_{n}"] for n in FIELDS}, z["met_levels"], z["met_p_hpa"], z["met_lon"],
                         z["met_lat"], float(z["met_t0"]))
     else:
-        spec = _c0_spec(int(z["met_seed"]))
+        case = str(z["met_case"]) if "met_case" in z else "c0"
+        spec = config_met_spec(1, n_snapshots=4) if case == "c1" else _c0_spec(int(z["met_seed"]))
+        if spec.seed != int(z["met_seed"]):
+            raise RuntimeError(f"{name}: met seed {int(z['met_seed'])} does not match the {case} spec")
         met = met_from_synthetic(SyntheticMet(spec))
         chk = np.array([float(np.sum(met.fields[k], dtype=np.float64)) for k in FIELDS])
         if not np.allclose(chk, z["met_checksum"], rtol=1e-6, atol=1e-3):

@@ -16,7 +16,13 @@ synthetic met windows with ``glide_b200.synthetic``, and records:
   by a replica of the cursor loop ``main.py:1382-1477`` with injected noise.
 * ``run_c0.npz`` — a 3 h batch on the 64x64x40 smoke-case met with meander
   and convection off (the met is regenerated from its seed; a checksum of it
-  is stored).
+  is stored);
+* ``run_c1.npz`` — the single-site EUROPE-box workload (60x281x401 met, dt
+  30 s, meander and hourly convection on) for 20,000 particles of its release,
+  2 h backward from the release end (met regenerated from its seed).
+
+Every batch also records the runtime's per-step diagnostics (mean particle
+position, grid-mean wind; ``main.py:1565-1566``).
 
 Noise is not stored: it is regenerated from the recorded seed by
 ``tests/golden/noise.py``.
@@ -42,7 +48,7 @@ sys.path.insert(0, str(HERE))
 
 from noise import conv_uniforms, step_noise  # noqa: E402
 
-from glide_b200.synthetic import SyntheticMet, SyntheticMetSpec  # noqa: E402
+from glide_b200.synthetic import SyntheticMet, SyntheticMetSpec, config_met_spec  # noqa: E402
 
 
 def _import_reference(ref_root: Path):
@@ -51,7 +57,8 @@ def _import_reference(ref_root: Path):
     (stub_dir / "xarray" / "__init__.py").write_text(
         "class Dataset:\n    pass\n\n\nclass DataArray:\n    pass\n"
     )
-    sys.path.insert(0, str(ref_root / "src"))
+    # a source tree (src/lpdm) or an installed package directory (lpdm)
+    sys.path.insert(0, str(ref_root / "src") if (ref_root / "src" / "lpdm").is_dir() else str(ref_root))
     sys.path.insert(0, str(stub_dir))
     import os
 
@@ -189,6 +196,7 @@ class _NoiseShim:
         self.step = 0
         self.calls = 0
         self.meander_calls = 0
+        self.cached_step, self.cached = None, None
         self.orig = ref.ge.GPUEngine.update_langevin_velocity
         shim = self
 
@@ -196,13 +204,16 @@ class _NoiseShim:
             import torch
 
             if noise is None:
-                sub, mea = step_noise(shim.seed, shim.step, shim.max_substeps, shim.n)
+                if shim.cached_step != shim.step:  # one draw of the step's noise serves all its calls
+                    shim.cached = step_noise(shim.seed, shim.step, shim.max_substeps, shim.n)
+                    shim.cached_step = shim.step
+                sub, mea = shim.cached
                 if isinstance(t_lagrangian, float):
-                    noise = torch.from_numpy(mea[shim.meander_calls].copy())
+                    noise = torch.from_numpy(mea[shim.meander_calls].copy()).to(w_prime.device)
                     shim.meander_calls += 1
                 else:
                     i, c = divmod(shim.calls, 3)
-                    noise = torch.from_numpy(sub[i, c].copy())
+                    noise = torch.from_numpy(sub[i, c].copy()).to(w_prime.device)
                     shim.calls += 1
             return shim.orig(engine, w_prime, t_lagrangian, sigma_w2, dt_seconds, noise=noise, drift=drift)
 
@@ -232,7 +243,7 @@ class _RandShim:
             u1, u2 = conv_uniforms(shim.seed, shim.step, int(n))
             arr = (u1, u2)[shim.k]
             shim.k += 1
-            return torch.from_numpy(arr.copy())
+            return torch.from_numpy(arr.copy()).to(device if device is not None else "cpu")
 
         proxy = types.ModuleType("torch_proxy")
         proxy.__dict__.update({k: getattr(real_torch, k) for k in dir(real_torch) if not k.startswith("__")})
@@ -261,6 +272,20 @@ def _batch_setup(case: str):
         grid = dict(lon_bounds=(0.0, 5.75), lat_bounds=(40.0, 44.75), n_x=23, n_y=19, z_edges=(0.0, 100.0, 500.0),
                     n_time_bins=3)
         domain = dict(lon_bounds=(0.5, 5.25), lat_bounds=(40.5, 44.25), alt_max_m=6000.0)
+    elif case == "c1":
+        # the single-site EUROPE-box workload (60 x 281 x 401 met, dt 30 s, meander and hourly
+        # convection on): 20,000 particles of its 100 m release at (-5, 52) over a 1 h release
+        # window, run 2 h backward from the release end (every particle is 1-2 h old at the end)
+        spec = config_met_spec(1, n_snapshots=4)
+        t0 = spec.start_time
+        rel = [(-5.0, 52.0, 100.0, 20000, t0 + timedelta(hours=1), 3600.0)]
+        sim_length_s = 24 * 3600.0
+        dt_s = 30.0
+        meander, convection = True, True
+        grid = dict(lon_bounds=(-60.125, 40.125), lat_bounds=(9.875, 80.125), n_x=401, n_y=281,
+                    z_edges=(0.0, 100.0), n_time_bins=24)
+        domain = dict(lon_bounds=(-60.0, 40.0), lat_bounds=(10.0, 80.0), alt_max_m=20000.0)
+        return spec, rel, sim_length_s, dt_s, meander, convection, grid, domain, 2 * 3600.0
     else:
         spec = SyntheticMetSpec(nz=40, ny=64, nx=64, lon0=0.0, lat0=40.0, n_snapshots=5, moist_fraction=0.0,
                                 seed=20261203, start_time=datetime(2026, 1, 14, 23, tzinfo=UTC))
@@ -271,7 +296,7 @@ def _batch_setup(case: str):
         grid = dict(lon_bounds=(0.0, 16.0), lat_bounds=(40.0, 56.0), n_x=64, n_y=64, z_edges=(0.0, 100.0),
                     n_time_bins=3)
         domain = dict(lon_bounds=(0.0, 15.75), lat_bounds=(40.0, 55.75), alt_max_m=20000.0)
-    return spec, rel, sim_length_s, dt_s, meander, convection, grid, domain
+    return spec, rel, sim_length_s, dt_s, meander, convection, grid, domain, None
 
 
 def _particles(spec: SyntheticMetSpec, rel, seed: int):
@@ -294,40 +319,46 @@ def _particles(spec: SyntheticMetSpec, rel, seed: int):
             np.concatenate(ends).astype(np.float32), np.concatenate(ridx).astype(np.int64), batch_start)
 
 
-def make_run(ref, case: str, out_path: Path, noise_seed: int) -> None:
+def drive_batch(ref, case: str, noise_seed: int, device: str = "cpu", snap_every: int = 20) -> dict:
+    """Runs golden case ``case`` through the reference's static step path on ``device``
+    (its eager torch ops on the CPU or on CUDA), with the injected noise of ``noise_seed``,
+    driven by a replica of the cursor loop ``main.py:1382-1477``; returns the fixture's
+    arrays (inputs, run configuration and outputs)."""
     import torch
 
-    spec, rel, sim_length_s, dt_s, meander, convection, grid, domain = _batch_setup(case)
+    dev = torch.device(device)
+    spec, rel, sim_length_s, dt_s, meander, convection, grid, domain, run_s = _batch_setup(case)
     syn = SyntheticMet(spec)
     particles, rel_off, win_end, ridx, batch_start = _particles(spec, rel, noise_seed + 1)
     n = particles.shape[1]
     max_substeps = 6
     window_ends = [r[4] + timedelta(seconds=r[5]) for r in rel]
     cursor_start = max(window_ends)
-    terminus = min(window_ends) - timedelta(seconds=sim_length_s)
+    terminus = min(window_ends) - timedelta(seconds=sim_length_s if run_s is None else run_s)
 
     scheme = ref.hn.HannaScheme(meander_enabled=meander, static_substeps=True, max_substeps=max_substeps)
     conv_scheme = ref.em.EmanuelReducedConvection() if convection else None
-    engine = ref.ge.GPUEngine(device="cpu")
+    engine = ref.ge.GPUEngine(device=str(dev))
     gridder = ref.fg.FootprintGridder(lon_bounds=grid["lon_bounds"], lat_bounds=grid["lat_bounds"],
                                       z_edges_m=grid["z_edges"], n_time_bins=grid["n_time_bins"],
-                                      n_y=grid["n_y"], n_x=grid["n_x"], n_releases=len(rel), device="cpu")
+                                      n_y=grid["n_y"], n_x=grid["n_x"], n_releases=len(rel), device=dev)
     cfg = SimpleNamespace(met_domain=SimpleNamespace(**domain))
     shim = _NoiseShim(ref, noise_seed, n, max_substeps)
     rshim = _RandShim(ref, noise_seed + 7) if convection else None
-    p = torch.from_numpy(particles.T.copy())
-    rel_t = torch.from_numpy(rel_off)
-    end_t = torch.from_numpy(win_end)
-    ridx_t = torch.from_numpy(ridx)
-    state = scheme.initialize_state(n, device=torch.device("cpu"), dtype=torch.float32)
-    alive = torch.ones(n, dtype=torch.bool)
+    p = torch.from_numpy(particles.T.copy()).to(dev)
+    rel_t = torch.from_numpy(rel_off).to(dev)
+    end_t = torch.from_numpy(win_end).to(dev)
+    ridx_t = torch.from_numpy(ridx).to(dev)
+    state = scheme.initialize_state(n, device=dev, dtype=torch.float32)
+    alive = torch.ones(n, dtype=torch.bool, device=dev)
     windows: dict = {}
     last_bracket = None
     wind_cache: dict = {}
-    esc, act, conv_log, snaps = [], [], [], []
+    esc, act, conv_log, snaps, diag_pos, diag_wind = [], [], [], [], [], []
     t_cursor = cursor_start
     step = 0
     bstart = batch_start.timestamp()
+    host = lambda t: t.detach().cpu().numpy()  # noqa: E731
     try:
         while t_cursor > terminus:
             delta = min(dt_s, (t_cursor - terminus).total_seconds())
@@ -337,8 +368,8 @@ def make_run(ref, case: str, out_path: Path, noise_seed: int) -> None:
             if h not in windows:
                 windows[h] = _ref_window(ref, syn, h)
             win = windows[h]
-            alpha, _ = ref.main._advection_alpha_wind_mean(win, t_cursor, delta, torch.device("cpu"), torch.float32,
-                                                           wind_cache)
+            alpha, wind_mean = ref.main._advection_alpha_wind_mean(win, t_cursor, delta, dev, torch.float32,
+                                                                   wind_cache)
             shim.begin_step(step)
             p, state = scheme.step(particles=p, state=state, met_window=win, t_alpha=alpha, dt_seconds=delta,
                                    active_mask=active, engine=engine)
@@ -360,8 +391,11 @@ def make_run(ref, case: str, out_path: Path, noise_seed: int) -> None:
             alive = alive & ~newly
             esc.append(int(newly.sum()))
             act.append(int(active.sum()))
-            if step % 20 == 0:
-                snaps.append((step, p.numpy().T.copy()))
+            # the per-step diagnostics of main.py:1565-1566
+            diag_pos.append(host(p[:, :3].mean(dim=0)).copy())
+            diag_wind.append(host(wind_mean).copy())
+            if step % snap_every == 0:
+                snaps.append((step, host(p).T.copy()))
             t_cursor = t_cursor - timedelta(seconds=delta)
             step += 1
     finally:
@@ -378,12 +412,13 @@ def make_run(ref, case: str, out_path: Path, noise_seed: int) -> None:
                grid_nxy=np.array([grid["n_x"], grid["n_y"], grid["n_time_bins"]]), grid_z=np.array(grid["z_edges"]),
                dom_lon=np.array(domain["lon_bounds"]), dom_lat=np.array(domain["lat_bounds"]),
                dom_alt=np.array(domain["alt_max_m"]),
-               out_particles=p.numpy().T.copy(), out_alive=alive.numpy(), out_footprint=gridder.tensor.numpy(),
+               out_particles=host(p).T.copy(), out_alive=host(alive), out_footprint=host(gridder.tensor),
                out_escaped=np.array(esc), out_active=np.array(act), out_conv=np.array(conv_log).reshape(-1, 2),
                snap_steps=np.array([s for s, _ in snaps]), snap_particles=np.stack([a for _, a in snaps]),
+               out_diag_pos=np.stack(diag_pos).astype(np.float32), out_diag_wind=np.stack(diag_wind).astype(np.float32),
                n_steps=np.array(step))
     for k, v in state.items():
-        out[f"out_{k}"] = v.numpy()
+        out[f"out_{k}"] = host(v)
     met = _met_arrays(syn)
     if case == "small":
         out.update(met)
@@ -391,18 +426,39 @@ def make_run(ref, case: str, out_path: Path, noise_seed: int) -> None:
         out["met_checksum"] = np.array([float(np.sum(met[f"met_{k}"], dtype=np.float64))
                                         for k in ("u", "v", "w", "t", "q", "blh", "sp", "ustar", "shf")])
         out["met_seed"] = np.array(spec.seed)
+        out["met_case"] = np.array(case)
+    return out
+
+
+# noise seed of each golden batch
+NOISE_SEEDS = {"small": 4242, "c0": 777, "c1": 9001}
+# snapshot interval (outer steps) of each golden batch
+SNAP_EVERY = {"small": 20, "c0": 20, "c1": 60}
+
+
+def make_run(ref, case: str, out_path: Path) -> None:
+    out = drive_batch(ref, case, NOISE_SEEDS[case], snap_every=SNAP_EVERY[case])
     np.savez_compressed(out_path, **out)
-    print("wrote", out_path, "steps", step, "escaped", sum(esc), "conv", conv_log)
+    print("wrote", out_path, "steps", int(out["n_steps"]), "escaped", int(out["out_escaped"].sum()),
+          "conv", out["out_conv"].tolist())
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference source tree (holds src/lpdm)")
+    ap.add_argument("--only", nargs="*", choices=["units", "small", "c0", "c1"],
+                    help="fixtures to (re)generate (default: all)")
     args = ap.parse_args()
     ref = _import_reference(Path(args.reference))
-    make_units(ref, HERE / "units.npz")
-    make_run(ref, "small", HERE / "run_small.npz", noise_seed=4242)
-    make_run(ref, "c0", HERE / "run_c0.npz", noise_seed=777)
+    want = set(args.only or ["units", "small", "c0", "c1"])
+    if "units" in want:
+        make_units(ref, HERE / "units.npz")
+    if "small" in want:
+        make_run(ref, "small", HERE / "run_small.npz")
+    if "c0" in want:
+        make_run(ref, "c0", HERE / "run_c0.npz")
+    if "c1" in want:
+        make_run(ref, "c1", HERE / "run_c1.npz")
 
 
 if __name__ == "__main__":

@@ -143,3 +143,49 @@ def test_batch_matches_reference(name):
     fp, rfp = res.footprint, run["out_footprint"]
     assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 5e-3
     assert abs(fp.sum() - rfp.sum()) / rfp.sum() < 1e-3
+
+
+def _diag_errors(res, run):
+    """(relative error of the mean-position diagnostic per step and coordinate against
+    max(|x|, 1), absolute error of the mean-wind diagnostic in m/s)."""
+    dp = np.asarray(res.diag_pos, dtype=np.float64)
+    gp = run["out_diag_pos"].astype(np.float64)
+    dw = np.asarray(res.diag_wind, dtype=np.float64)
+    return np.abs(dp - gp) / np.maximum(np.abs(gp), 1.0), np.abs(dw - run["out_diag_wind"])
+
+
+@pytest.mark.parametrize("name", ["run_small", "run_c0"])
+def test_diagnostics_match_reference(name):
+    """The per-step diagnostics of main.py:1565-1566: the grid-mean wind within float32
+    rounding of the reference's float32 grid means; the mean position equal at the first
+    step and within the batch's ensemble spread afterwards."""
+    run = load_run(name)
+    res = run_batch(**oracle_kwargs(run))
+    pos, wind = _diag_errors(res, run)
+    assert wind.max() < 5e-6, wind.max()
+    assert pos[0].max() < 1e-6, pos[0]
+    assert np.median(pos) < 1e-6
+    assert pos.max() < 1e-3, pos.max()
+
+
+def test_c1_batch_matches_reference():
+    """The single-site EUROPE-box case (60 x 281 x 401 met, dt 30 s, meander and hourly
+    convection on; 20,000 particles, 2 h): counts and the alive mask exact, 99.5 % of the
+    trajectories within 1e-5 relative of the reference after 2 h (measured 99.87 %), the
+    footprint within 1e-5 relative L1 (measured 7.7e-7), the diagnostics within 1e-6."""
+    run = load_run("run_c1")
+    res = run_batch(**oracle_kwargs(run))
+    assert res.n_steps == int(run["n_steps"])
+    assert np.array_equal(res.active_per_step, run["out_active"])
+    assert np.array_equal(res.escaped_per_step, run["out_escaped"])
+    assert np.array_equal(res.alive, run["out_alive"])
+    assert [m for _, f, m in res.convection] == [int(m) for _, m in run["out_conv"] if m > 0]
+    ref = run["out_particles"]
+    scale = np.maximum(np.abs(ref[:3]), np.array([[1.0], [1.0], [10.0]]))
+    err = (np.abs(res.particles[:3] - ref[:3]) / scale).max(axis=0)
+    assert np.mean(err < 1e-5) >= 0.995, np.mean(err < 1e-5)
+    fp, rfp = res.footprint.astype(np.float64), run["out_footprint"].astype(np.float64)
+    assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 1e-5
+    pos, wind = _diag_errors(res, run)
+    assert pos.max() < 1e-6, pos.max()
+    assert wind.max() < 5e-6, wind.max()
