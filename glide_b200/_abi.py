@@ -37,7 +37,7 @@ class WindowDesc(C.Structure):
                 ("blh", vp * 2), ("sp", vp * 2), ("ustar", vp * 2), ("shf", vp * 2), ("height3d", vp),
                 ("height_level", vp), ("pressure_hpa", vp), ("meander_coefficient", C.c_float),
                 ("meander_radius", C.c_int32), ("build_meander", C.c_int32), ("met_dtype", C.c_int32),
-                ("wind_packed", vp), ("surf_packed", vp), ("support_packed", vp)]
+                ("wind_packed", vp), ("surf_packed", vp), ("support_packed", vp), ("wind_sum", vp)]
 
 
 class StepSched(C.Structure):
@@ -47,7 +47,7 @@ class StepSched(C.Structure):
 class FootprintGrid(C.Structure):
     _fields_ = [("lon_min", C.c_double), ("lon_max", C.c_double), ("lat_min", C.c_double), ("lat_max", C.c_double),
                 ("n_releases", C.c_int32), ("n_time_bins", C.c_int32), ("n_z", C.c_int32), ("n_y", C.c_int32),
-                ("n_x", C.c_int32), ("z_edges", vp), ("ring", C.c_int32)]
+                ("n_x", C.c_int32), ("z_edges", vp), ("ring", C.c_int32), ("value_f64", C.c_int32)]
 
 
 class StepArgs(C.Structure):
@@ -64,7 +64,7 @@ class StepArgs(C.Structure):
                 ("dom_lat_min", C.c_double), ("dom_lat_max", C.c_double), ("dom_alt_max", C.c_double),
                 ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32),
                 ("order", vp), ("work_key", vp), ("conv_column", vp), ("conv_step", C.c_int32),
-                ("conv_nz", C.c_int32), ("conv_uniforms", vp), ("conv_moved", vp)]
+                ("conv_nz", C.c_int32), ("conv_uniforms", vp), ("conv_moved", vp), ("diag_pos_sum", vp)]
 
 
 class ConvectArgs(C.Structure):
@@ -93,7 +93,8 @@ class RegridArgs(C.Structure):
 class CompactArgs(C.Structure):
     _fields_ = [("rows", vp), ("n_rows", C.c_int64), ("cells", C.c_int64), ("row_index", vp), ("k", C.c_int32),
                 ("clear", C.c_int32), ("slice_offset", vp), ("out_cell", vp), ("out_value", vp),
-                ("capacity", C.c_int64), ("status", vp), ("scratch", vp), ("scratch_bytes", C.c_size_t)]
+                ("capacity", C.c_int64), ("status", vp), ("scratch", vp), ("scratch_bytes", C.c_size_t),
+                ("value_f64", C.c_int32)]
 
 
 STRUCTS = (Grid, WindowDesc, StepSched, FootprintGrid, StepArgs, ConvectArgs, OuArgs, RegridArgs, CompactArgs)

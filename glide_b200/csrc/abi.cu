@@ -29,7 +29,7 @@ glide_status check_launch(const char* what) {
 
 }  // namespace glide
 
-extern "C" int32_t glide_version(void) { return 100; /* 0.1.0 */ }
+extern "C" int32_t glide_version(void) { return 200; /* 0.2.0 */ }
 
 extern "C" glide_status glide_last_error(char* buf, size_t len) {
     if (!buf || len == 0) return GLIDE_ERR_INVALID_ARG;

@@ -1,5 +1,6 @@
 // Sparse form of completed footprint slices: (cell, value) lists of the cells whose
-// float32 bit pattern is not zero, slices in the caller's order, cells ascending.
+// float32 (or float64) bit pattern is not zero, slices in the caller's order, cells
+// ascending.
 //
 // A slice (one release's time_ago bin, Zb x Y x X float32) of a backward plume is
 // mostly zero: the plume of one release covers a few thousand of the 1.1e5 cells of
@@ -26,8 +27,10 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kItems = 8;
 constexpr int kTile = kThreads * kItems;
 
+// W: the value word, uint32_t (float32 footprints) or unsigned long long (float64)
+template <typename W>
 __global__ void __launch_bounds__(kThreads)
-    compact_count(const uint32_t* __restrict__ rows, int64_t n_rows, int64_t cells,
+    compact_count(const W* __restrict__ rows, int64_t n_rows, int64_t cells,
                   const int64_t* __restrict__ row_index, int64_t tiles, int32_t* __restrict__ count,
                   uint32_t* status) {
     __shared__ int32_t warp_n[kWarps];
@@ -36,12 +39,12 @@ __global__ void __launch_bounds__(kThreads)
     const int64_t row = row_index[s];
     int32_t c = 0;
     if (row >= 0 && row < n_rows) {
-        const uint32_t* src = rows + row * cells;
+        const W* src = rows + row * cells;
         const int64_t t0 = t * kTile;
 #pragma unroll
         for (int r = 0; r < kItems; ++r) {
             const int64_t i = t0 + (int64_t)r * kThreads + threadIdx.x;
-            if (i < cells) c += src[i] != 0u ? 1 : 0;
+            if (i < cells) c += src[i] != W(0) ? 1 : 0;
         }
     } else if (t == 0 && threadIdx.x == 0 && status) {
         atomicOr(status, (uint32_t)GLIDE_STATUS_BAD_ROW);
@@ -86,10 +89,11 @@ __global__ void __launch_bounds__(1024)
     for (int64_t j = threadIdx.x; j <= k; j += 1024) slice_offset[j] = offset[j * tiles];
 }
 
+template <typename W>
 __global__ void __launch_bounds__(kThreads)
-    compact_write(uint32_t* __restrict__ rows, int64_t n_rows, int64_t cells, const int64_t* __restrict__ row_index,
+    compact_write(W* __restrict__ rows, int64_t n_rows, int64_t cells, const int64_t* __restrict__ row_index,
                   int64_t tiles, const int64_t* __restrict__ offset, int64_t m, int64_t capacity, int clear,
-                  int32_t* __restrict__ out_cell, uint32_t* __restrict__ out_value, uint32_t* status) {
+                  int32_t* __restrict__ out_cell, W* __restrict__ out_value, uint32_t* status) {
     __shared__ int32_t warp_n[kWarps];
     // both conditions below are the same for every thread of the block: it returns as a whole
     const int64_t total = offset[m];
@@ -101,7 +105,7 @@ __global__ void __launch_bounds__(kThreads)
     const int64_t s = blk / tiles, t = blk - s * tiles;
     const int64_t row = row_index[s];
     if (row < 0 || row >= n_rows) return;  // counted as an empty slice
-    uint32_t* src = rows + row * cells;
+    W* src = rows + row * cells;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t0 = t * kTile;
     int64_t base = offset[blk];
@@ -109,8 +113,8 @@ __global__ void __launch_bounds__(kThreads)
         // the items of round r are cells t0 + r * kThreads + [0, kThreads): in cell order
         // across the warps of the block, so rounds in sequence keep the tile in cell order
         const int64_t i = t0 + (int64_t)r * kThreads + threadIdx.x;
-        const uint32_t bits = i < cells ? src[i] : 0u;
-        const unsigned ball = __ballot_sync(0xffffffffu, bits != 0u);
+        const W bits = i < cells ? src[i] : W(0);
+        const unsigned ball = __ballot_sync(0xffffffffu, bits != W(0));
         if (lane == 0) warp_n[w] = __popc(ball);
         __syncthreads();
         int32_t before = 0, all = 0;
@@ -120,13 +124,13 @@ __global__ void __launch_bounds__(kThreads)
             before += ww < w ? c : 0;
             all += c;
         }
-        if (bits != 0u) {
+        if (bits != W(0)) {
             const int64_t o = base + before + __popc(ball & ((1u << lane) - 1u));
             if (o < capacity) {
                 out_cell[o] = (int32_t)i;
                 out_value[o] = bits;
             }
-            if (clear) src[i] = 0u;
+            if (clear) src[i] = W(0);
         }
         base += all;
         __syncthreads();  // warp_n is rewritten by the next round
@@ -136,6 +140,19 @@ __global__ void __launch_bounds__(kThreads)
 int64_t tiles_of(int64_t cells) { return (cells + kTile - 1) / kTile; }
 
 bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; }
+
+template <typename W>
+void launch_compact(const glide_compact_args* a, W* rows, int64_t tiles, int64_t m, int64_t* offset, int32_t* count,
+                    cudaStream_t s) {
+    if (m > 0)
+        compact_count<W><<<(unsigned)m, kThreads, 0, s>>>(rows, a->n_rows, a->cells, a->row_index, tiles, count,
+                                                           a->status);
+    compact_scan<<<1, 1024, 0, s>>>(count, m, tiles, a->k, offset, a->slice_offset);
+    if (m > 0)
+        compact_write<W><<<(unsigned)m, kThreads, 0, s>>>(rows, a->n_rows, a->cells, a->row_index, tiles, offset, m,
+                                                           a->capacity, a->clear != 0, a->out_cell,
+                                                           static_cast<W*>(a->out_value), a->status);
+}
 
 }  // namespace
 }  // namespace glide
@@ -173,22 +190,16 @@ extern "C" glide_status glide_footprint_compact(const glide_compact_args* a, voi
     if (a->scratch_bytes < need)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_compact: scratch is %zu bytes, %zu needed",
                          a->scratch_bytes, need);
+    const uintptr_t word = a->value_f64 ? 8 : 4;
     if (!aligned(a->scratch, 8) || !aligned(a->slice_offset, 8) || !aligned(a->row_index, 8) ||
-        !aligned(a->rows, 4) || !aligned(a->out_cell, 4) || !aligned(a->out_value, 4) || !aligned(a->status, 4))
+        !aligned(a->rows, word) || !aligned(a->out_cell, 4) || !aligned(a->out_value, word) || !aligned(a->status, 4))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_compact: misaligned pointer");
     const int64_t tiles = tiles_of(a->cells);
     const int64_t m = (int64_t)a->k * tiles;
     cudaStream_t s = (cudaStream_t)stream;
     int64_t* offset = static_cast<int64_t*>(a->scratch);
     int32_t* count = reinterpret_cast<int32_t*>(offset + m + 1);
-    uint32_t* rows = reinterpret_cast<uint32_t*>(a->rows);
-    if (m > 0)
-        compact_count<<<(unsigned)m, kThreads, 0, s>>>(rows, a->n_rows, a->cells, a->row_index, tiles, count,
-                                                        a->status);
-    compact_scan<<<1, 1024, 0, s>>>(count, m, tiles, a->k, offset, a->slice_offset);
-    if (m > 0)
-        compact_write<<<(unsigned)m, kThreads, 0, s>>>(rows, a->n_rows, a->cells, a->row_index, tiles, offset, m,
-                                                        a->capacity, a->clear != 0, a->out_cell,
-                                                        reinterpret_cast<uint32_t*>(a->out_value), a->status);
+    if (a->value_f64) launch_compact(a, static_cast<unsigned long long*>(a->rows), tiles, m, offset, count, s);
+    else launch_compact(a, static_cast<uint32_t*>(a->rows), tiles, m, offset, count, s);
     return check_launch("glide_footprint_compact");
 }

@@ -402,14 +402,22 @@ static __device__ __align__(256) double g_convect_scratch[8 + 4 * NOALLOC_MAX_NZ
 static std::mutex g_scratch_mu;
 static double* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
 
-static glide_status noalloc_scratch(double** out) {
+// The device address of g_convect_scratch on the current device. Looked up with
+// cudaGetSymbolAddress on every call made outside stream capture (so the address
+// follows the module if the device's context was reset and the library's module
+// loaded again); a call on a capturing stream uses the address the last
+// uncaptured call on that device found.
+static glide_status noalloc_scratch(cudaStream_t stream, double** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_error(e, "glide_convect_noalloc: cudaGetDevice");
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
         return set_error(GLIDE_ERR_UNSUPPORTED, "glide_convect_noalloc: device ordinal %d out of range", dev);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(stream, &cs);
+    if (e != cudaSuccess) return cuda_error(e, "glide_convect_noalloc: cudaStreamIsCapturing");
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_convect_scratch);
         if (e != cudaSuccess) return cuda_error(e, "glide_convect_noalloc: cudaGetSymbolAddress");
@@ -436,7 +444,7 @@ extern "C" glide_status glide_convect_noalloc(const glide_convect_args* a, void*
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: NULL particle input");
     if (a->z_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_convect_noalloc: z_stride < 1");
     double* scratch = nullptr;
-    const glide_status st = noalloc_scratch(&scratch);
+    const glide_status st = noalloc_scratch((cudaStream_t)stream, &scratch);
     if (st != GLIDE_OK) return st;
     ConvDev d;
     d.n = a->n; d.z = a->z; d.zs = a->z_stride;

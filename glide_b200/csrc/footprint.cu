@@ -15,14 +15,17 @@ struct FpDev {
     float lon0, lon_span, lat0, lat_span;
     int R, T, Z, Y, X;
     const float* edges;
-    float* fp;
+    void* fp;
 };
 
+// V = float: the float32 gridder (w_eff = weight * dt in float32); V = double: the
+// float64 gridder (weight * dt formed and summed in FP64)
+template <typename V>
 __global__ void footprint_kernel(const FpDev d) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = false;
     int64_t flat = -1;
-    float w_eff = 0.0f;
+    V w_eff = 0;
     if (i < d.n && (!d.active || d.active[i])) {
         const float lon = d.lon[i * d.ps], lat = d.lat[i * d.ps], z = d.z[i * d.ps];
         const float xf = floorf(((lon - d.lon0) / d.lon_span) * (float)d.X);
@@ -35,20 +38,20 @@ __global__ void footprint_kernel(const FpDev d) {
                 (zb >= 0) && (zb < d.Z) && (tb >= 0) && (tb < d.T);
         if (valid) {
             flat = ((((int64_t)r * d.T + tb) * d.Z + zb) * d.Y + (int64_t)yf) * d.X + (int64_t)xf;
-            w_eff = d.w[i * d.ws] * d.dt;
+            w_eff = (V)d.w[i * d.ws] * (V)d.dt;
         }
     }
     const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     if (valid) {
         const unsigned peers = __match_any_sync(vmask, (unsigned long long)flat);
-        float sum = 0.0f;
+        V sum = 0;
         unsigned m = peers;
         while (m) {
             const int src = __ffs(m) - 1;
             m &= m - 1;
             sum += __shfl_sync(peers, w_eff, src);
         }
-        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(d.fp + flat, sum);
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(static_cast<V*>(d.fp) + flat, sum);
     }
 }
 
@@ -60,7 +63,7 @@ extern "C" glide_status glide_footprint_accumulate(int64_t n, const float* lon, 
                                                    int64_t pos_stride, const uint8_t* active, const float* weights,
                                                    int64_t weight_stride, const int32_t* t_idx,
                                                    const int32_t* release_idx, float dt_seconds,
-                                                   const glide_footprint_grid* g, float* footprint, void* stream) {
+                                                   const glide_footprint_grid* g, void* footprint, void* stream) {
     if (n < 0) return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: n < 0");
     if (n == 0) return GLIDE_OK;
     if (!lon || !lat || !z || !weights || !t_idx || !g || !footprint || !g->z_edges)
@@ -71,6 +74,8 @@ extern "C" glide_status glide_footprint_accumulate(int64_t n, const float* lon, 
         return set_error(GLIDE_ERR_UNSUPPORTED, "glide_footprint_accumulate: ring layout is only for glide_step");
     if (pos_stride < 1 || weight_stride < 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: stride < 1");
+    if (g->value_f64 && ((uintptr_t)footprint & 7u))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_footprint_accumulate: float64 footprint not 8-byte aligned");
     FpDev d;
     d.n = n; d.lon = lon; d.lat = lat; d.z = z; d.ps = pos_stride;
     d.active = active; d.w = weights; d.ws = weight_stride; d.t_idx = t_idx; d.rid = release_idx;
@@ -80,6 +85,8 @@ extern "C" glide_status glide_footprint_accumulate(int64_t n, const float* lon, 
     d.R = g->n_releases; d.T = g->n_time_bins; d.Z = g->n_z; d.Y = g->n_y; d.X = g->n_x;
     d.edges = g->z_edges; d.fp = footprint;
     const int threads = 256;
-    footprint_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(d);
+    const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+    if (g->value_f64) footprint_kernel<double><<<blocks, threads, 0, (cudaStream_t)stream>>>(d);
+    else footprint_kernel<float><<<blocks, threads, 0, (cudaStream_t)stream>>>(d);
     return check_launch("glide_footprint_accumulate");
 }

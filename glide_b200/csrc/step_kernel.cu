@@ -55,7 +55,7 @@ struct StepDev {
     const glide_step_sched* sched; glide_step_sched sched0;
     int n_steps, phys_begin, post_begin;
     const float* noise_sub; const float* noise_mea; uint32_t seed_lo, seed_hi;
-    float* fp;
+    void* fp; int fp64;
     float fp_lon0, fp_lon_span, fp_lat0, fp_lat_span;
     int fp_R, fp_T, fp_Z, fp_Y, fp_X, fp_ring;
     const float* fp_edges;
@@ -64,7 +64,51 @@ struct StepDev {
     uint32_t* status;
     const int32_t* order; uint8_t* work_key;
     const double* conv_column; int conv_step, conv_nz; const float* conv_uniforms; int32_t* conv_moved;
+    double* diag;
 };
+
+// Dynamic shared memory of one block: when the launch sums the position diagnostic,
+// [3] float64 position sums of the block's idle warps (constant over the launch) and
+// [n_steps][3] float64 position sums of the others; then [2][n_steps] int32 escaped /
+// active counts.
+__host__ __device__ inline size_t step_smem_bytes(int n_steps, bool diag) {
+    return (diag ? sizeof(double) * 3 * (size_t)(n_steps + 1) : 0) + sizeof(int32_t) * 2 * (size_t)n_steps;
+}
+
+// Sum of v over the 32 lanes of a converged warp, in every lane.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Smallest and largest cursor offset of the launch's steps, in every lane of the warp.
+__device__ __forceinline__ void launch_cursor_range(const StepDev& p, int lane, float& lo, float& hi) {
+    if (!p.sched) {
+        lo = hi = p.sched0.cursor_off;
+        return;
+    }
+    float mn = INFINITY, mx = -INFINITY;
+    for (int j = lane; j < p.n_steps; j += 32) {
+        const float c = p.sched[j].cursor_off;
+        mn = fminf(mn, c);
+        mx = fmaxf(mx, c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    lo = mn;
+    hi = mx;
+}
+
+// One footprint cell's residence time accumulated in a register, added to the
+// footprint (float32 or float64 values) with one atomic.
+__device__ __forceinline__ void footprint_flush(const StepDev& p, int64_t cell, double acc) {
+    if (p.fp64) atomicAdd(static_cast<double*>(p.fp) + cell, acc);
+    else atomicAdd(static_cast<float*>(p.fp) + cell, (float)acc);
+}
 
 // ---------------------------------------------------------------------------
 // Hanna column turbulence (hanna.py:192-337, 1500-1596)
@@ -273,7 +317,10 @@ constexpr int kNumVariants = kNumShapes + 1;
 // The whole launch body for one batch; `block` is the block's index within the batch.
 template <typename T, bool GENERAL>
 __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
-    extern __shared__ int32_t s_counts[];  // [2][n_steps]: escaped, active
+    extern __shared__ double s_dyn[];
+    double* const s_static = s_dyn;     // [3] when p.diag
+    double* const s_diag = s_dyn + 3;   // [n_steps][3] when p.diag
+    int32_t* const s_counts = reinterpret_cast<int32_t*>(s_dyn + (p.diag ? 3 * (p.n_steps + 1) : 0));  // [2][n_steps]
     const int64_t th = block * blockDim.x + threadIdx.x;
     bool have = th < p.n;
     bool bad_order = false;
@@ -285,6 +332,8 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
     }
     const int lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < 2 * p.n_steps; k += blockDim.x) s_counts[k] = 0;
+    if (p.diag)
+        for (int k = threadIdx.x; k < 3 * (p.n_steps + 1); k += blockDim.x) s_dyn[k] = 0.0;
     __syncthreads();
 
     float lon = 0.f, lat = 0.f, z = 0.f, wgt = 0.f, up = 0.f, vp = 0.f, wp = 0.f, um = 0.f, vm = 0.f;
@@ -309,285 +358,326 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
     const int ms = p.max_substeps;
     bool nonfinite = false;
     // footprint cache: a particle stays in one output cell for many steps, so its
-    // residence time accumulates in a register and goes to global memory (one
+    // residence time accumulates in a register (FP64) and goes to global memory (one
     // atomic) only when the cell (or time bin) changes, and at the end of the launch
     int64_t fp_cell = -1;
-    float fp_acc = 0.0f;
+    double fp_acc = 0.0;
     int last_k = 1;         // work class of the last physics step (work key)
     bool last_active = false;
 
-    for (int j = 0; j < p.n_steps; ++j) {
-        const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
-        bool active;
-        if (GENERAL && p.active_mask) active = have && p.active_mask[i] != 0;
-        else active = have && alive && (rel >= sc.cursor_off) && ((rel - L_sim) <= sc.cursor_off);
-        last_active = active;
+    // A warp whose particles are all inactive at every step of the launch (absent,
+    // escaped, past the simulation length at the launch's latest cursor, or not yet
+    // released at its earliest) has nothing to step: it skips the step loop, adds its
+    // unchanged positions to the diagnostic once for all steps, and writes its keys.
+    bool idle_warp = false;
+    if (!(GENERAL && p.active_mask)) {
+        float c_lo, c_hi;
+        launch_cursor_range(p, lane, c_lo, c_hi);
+        const bool idle = !have || !alive || ((rel - L_sim) > c_hi) || !(rel >= c_lo);
+        idle_warp = __all_sync(0xffffffffu, idle);
+    }
+    if (idle_warp) {
+        if (p.diag) {
+            const double sx = warp_sum(have ? (double)lon : 0.0);
+            const double sy = warp_sum(have ? (double)lat : 0.0);
+            const double sz = warp_sum(have ? (double)z : 0.0);
+            if (lane == 0) {
+                atomicAdd(&s_static[0], sx);
+                atomicAdd(&s_static[1], sy);
+                atomicAdd(&s_static[2], sz);
+            }
+        }
+        if (have && p.work_key) {
+            const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
+            p.work_key[i] = (uint8_t)((alive && !(rel >= sl.cursor_off)) ? GLIDE_WORK_PENDING : GLIDE_WORK_DONE);
+        }
+    } else {
+        for (int j = 0; j < p.n_steps; ++j) {
+            const glide_step_sched sc = p.sched ? p.sched[j] : p.sched0;
+            bool active;
+            if (GENERAL && p.active_mask) active = have && p.active_mask[i] != 0;
+            else active = have && alive && (rel >= sc.cursor_off) && ((rel - L_sim) <= sc.cursor_off);
+            last_active = active;
 
-        if (j >= p.phys_begin && active) {
-            const float delta = sc.delta, alpha = sc.alpha;
-            // --- RK2 midpoint advection, backward (hanna.py:855-896), then the support
-            // brick at z_eval. One sampling loop serves all three trilinear samples (one
-            // copy of the level search and gather in the code): stage 0 the wind at the
-            // start point, stage 1 at the midpoint (hanna.py:866-889, two snapshots lerped
-            // by alpha), stage 2 the support brick (FT sigma_w / T_Lw, rho, drho/dz,
-            // meander sigmas) at the advected position and z_eval = max(z, z_ubl).
-            const GridDev& g = p.g;
-            const float z_ubl = p.z_ubl;
-            float acc[6];
-            float ix, iy;
-            {
-                const float hd = 0.5f * delta;
-                float qx = lon, qy = lat, qz = z;
+            if (j >= p.phys_begin && active) {
+                const float delta = sc.delta, alpha = sc.alpha;
+                // --- RK2 midpoint advection, backward (hanna.py:855-896), then the support
+                // brick at z_eval. One sampling loop serves all three trilinear samples (one
+                // copy of the level search and gather in the code): stage 0 the wind at the
+                // start point, stage 1 at the midpoint (hanna.py:866-889, two snapshots lerped
+                // by alpha), stage 2 the support brick (FT sigma_w / T_Lw, rho, drho/dz,
+                // meander sigmas) at the advected position and z_eval = max(z, z_ubl).
+                const GridDev& g = p.g;
+                const float z_ubl = p.z_ubl;
+                float acc[6];
+                float ix, iy;
+                {
+                    const float hd = 0.5f * delta;
+                    float qx = lon, qy = lat, qz = z;
 #pragma unroll 1
-                for (int stage = 0; stage < 3; ++stage) {
-                    sample6<T>(static_cast<const T*>(stage < 2 ? p.wind : p.support), g, qx, qy, qz, acc, ix, iy);
-                    if (stage < 2) {
-                        const float om = 1.0f - alpha;
-                        const float u = acc[0] * om + acc[3] * alpha;
-                        const float vv = acc[1] * om + acc[4] * alpha;
-                        const float w = acc[2] * om + acc[5] * alpha;
-                        const float vx = u / m_per_deg_lon(qy);
-                        const float vy = div_known(vv, M_PER_DEG_LAT, INV_M_PER_DEG_LAT);
-                        if (stage == 0) {
-                            qx = lon - hd * vx;
-                            qy = lat - hd * vy;
-                            qz = z - hd * w;
-                        } else {
-                            lon = lon - delta * vx;
-                            lat = lat - delta * vy;
-                            z = z - delta * w;
-                            qx = lon;
-                            qy = lat;
-                            qz = fmaxf(z, z_ubl);
+                    for (int stage = 0; stage < 3; ++stage) {
+                        sample6<T>(static_cast<const T*>(stage < 2 ? p.wind : p.support), g, qx, qy, qz, acc, ix, iy);
+                        if (stage < 2) {
+                            const float om = 1.0f - alpha;
+                            const float u = acc[0] * om + acc[3] * alpha;
+                            const float vv = acc[1] * om + acc[4] * alpha;
+                            const float w = acc[2] * om + acc[5] * alpha;
+                            const float vx = u / m_per_deg_lon(qy);
+                            const float vy = div_known(vv, M_PER_DEG_LAT, INV_M_PER_DEG_LAT);
+                            if (stage == 0) {
+                                qx = lon - hd * vx;
+                                qy = lat - hd * vy;
+                                qz = z - hd * w;
+                            } else {
+                                lon = lon - delta * vx;
+                                lat = lat - delta * vy;
+                                z = z - delta * w;
+                                qx = lon;
+                                qy = lat;
+                                qz = fmaxf(z, z_ubl);
+                            }
                         }
                     }
                 }
-            }
-            const float z_eval = fmaxf(z, z_ubl);
-            const float ft_sw = acc[0], ft_tl = acc[1];
-            const float rho_p = acc[2];
-            const float drho_p = acc[3] * Scales<T>::drho;
-            const float m_su = acc[4], m_sv = acc[5];
+                const float z_eval = fmaxf(z, z_ubl);
+                const float ft_sw = acc[0], ft_tl = acc[1];
+                const float rho_p = acc[2];
+                const float drho_p = acc[3] * Scales<T>::drho;
+                const float m_su = acc[4], m_sv = acc[5];
 
-            // --- surface fields and stability (hanna.py:950-966, 142-189)
-            float sf[5];
-            surface_at<T>(p, lon, lat, alpha, sf);
-            Surface S;
-            S.blh = fmaxf(sf[0], BLH_MIN);
-            const float sp_ = sf[1];
-            S.ustar = fmaxf(sf[2], USTAR_MIN);
-            const float shf = sf[3], ts = sf[4];
-            {
-                const float rho = sp_ / (R_DRY * ts);
-                const float denom = (float)(0.4 * GRAVITY_D) * shf;
-                const float num = -(S.ustar * S.ustar * S.ustar) * ts * rho * C_P;
-                S.L = (fabsf(denom) > 1e-10f) ? num / denom : INFINITY;
-                S.hL = S.blh / S.L;
-                const float cube = ((GRAVITY * S.blh) * shf) / ((ts * rho) * C_P);
-                S.w_star = (cube > 0.0f) ? powf(fmaxf(cube, 0.0f), 1.0f / 3.0f) : 0.0f;
-                const float f_cor = (float)(2.0 * OMEGA_D) * sinf(lat * DEG2RAD);
-                S.f_abs = fmaxf(fabsf(f_cor), 1e-5f);
-            }
+                // --- surface fields and stability (hanna.py:950-966, 142-189)
+                float sf[5];
+                surface_at<T>(p, lon, lat, alpha, sf);
+                Surface S;
+                S.blh = fmaxf(sf[0], BLH_MIN);
+                const float sp_ = sf[1];
+                S.ustar = fmaxf(sf[2], USTAR_MIN);
+                const float shf = sf[3], ts = sf[4];
+                {
+                    const float rho = sp_ / (R_DRY * ts);
+                    const float denom = (float)(0.4 * GRAVITY_D) * shf;
+                    const float num = -(S.ustar * S.ustar * S.ustar) * ts * rho * C_P;
+                    S.L = (fabsf(denom) > 1e-10f) ? num / denom : INFINITY;
+                    S.hL = S.blh / S.L;
+                    const float cube = ((GRAVITY * S.blh) * shf) / ((ts * rho) * C_P);
+                    S.w_star = (cube > 0.0f) ? powf(fmaxf(cube, 0.0f), 1.0f / 3.0f) : 0.0f;
+                    const float f_cor = (float)(2.0 * OMEGA_D) * sinf(lat * DEG2RAD);
+                    S.f_abs = fmaxf(fabsf(f_cor), 1e-5f);
+                }
 
-            // --- sigma_w: the BL profile's at z_eval (column turbulence) and the closure's
-            // at z_eval +- 1 m for the well-mixed drift (hanna.py:984-991; above the BL the
-            // free-troposphere value from the support brick's channel 0). One rolled loop
-            // keeps one copy of the regime code.
-            const int sl = GENERAL ? p.sl_override : 0;
-            const float z_hi = z_eval + 1.0f;
-            const float z_lo = fmaxf(z_eval - 1.0f, z_ubl);
-            float sw_col = 0.f, sw_hi = 0.f, sw_lo = 0.f;
+                // --- sigma_w: the BL profile's at z_eval (column turbulence) and the closure's
+                // at z_eval +- 1 m for the well-mixed drift (hanna.py:984-991; above the BL the
+                // free-troposphere value from the support brick's channel 0). One rolled loop
+                // keeps one copy of the regime code.
+                const int sl = GENERAL ? p.sl_override : 0;
+                const float z_hi = z_eval + 1.0f;
+                const float z_lo = fmaxf(z_eval - 1.0f, z_ubl);
+                float sw_col = 0.f, sw_hi = 0.f, sw_lo = 0.f;
 #pragma unroll 1
-            for (int q = 0; q < 3; ++q) {
-                const float zq = q == 0 ? z_eval : (q == 1 ? z_hi : z_lo);
-                float s = bl_sigma_w(zq, S, q == 0 ? 0 : sl);
-                if (q > 0 && zq > S.blh) {
-                    const float izq = unnorm(norm_z(zq, g), g.zmax_idx);
-                    Tri tq;
-                    tri_weights(ix, iy, izq, g.nx, g.ny, g.nz, tq);
-                    const T* sup = static_cast<const T*>(p.support);
-                    float a = 0.f;
+                for (int q = 0; q < 3; ++q) {
+                    const float zq = q == 0 ? z_eval : (q == 1 ? z_hi : z_lo);
+                    float s = bl_sigma_w(zq, S, q == 0 ? 0 : sl);
+                    if (q > 0 && zq > S.blh) {
+                        const float izq = unnorm(norm_z(zq, g), g.zmax_idx);
+                        Tri tq;
+                        tri_weights(ix, iy, izq, g.nx, g.ny, g.nz, tq);
+                        const T* sup = static_cast<const T*>(p.support);
+                        float a = 0.f;
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const int zz = (c & 4) ? tq.z1 : tq.z0;
-                        const int yy = (c & 2) ? tq.y1 : tq.y0;
-                        const int xx = (c & 1) ? tq.x1 : tq.x0;
-                        a = a + to_f(sup[cell_index(zz, yy, xx, g.ny, g.nx) * 8]) * tq.w[c];
+                        for (int c = 0; c < 8; ++c) {
+                            const int zz = (c & 4) ? tq.z1 : tq.z0;
+                            const int yy = (c & 2) ? tq.y1 : tq.y0;
+                            const int xx = (c & 1) ? tq.x1 : tq.x0;
+                            a = a + to_f(sup[cell_index(zz, yy, xx, g.ny, g.nx) * 8]) * tq.w[c];
+                        }
+                        s = a;
                     }
-                    s = a;
+                    if (q == 0) sw_col = s;
+                    else if (q == 1) sw_hi = fmaxf(s, SIGMA_MIN);
+                    else sw_lo = fmaxf(s, SIGMA_MIN);
                 }
-                if (q == 0) sw_col = s;
-                else if (q == 1) sw_hi = fmaxf(s, SIGMA_MIN);
-                else sw_lo = fmaxf(s, SIGMA_MIN);
-            }
 
-            // --- column turbulence at z_eval (hanna.py:976-982)
-            Sig6 col = bl_profile(z_eval, S, sl, p.floors, sw_col);
-            if (z_eval > S.blh) {
-                col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
-                col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
-            }
-            const float su = fmaxf(col.su, SIGMA_MIN), sv = fmaxf(col.sv, SIGMA_MIN), sw = fmaxf(col.sw, SIGMA_MIN);
-            const float tlu = fmaxf(col.tlu, T_L_MIN), tlv = fmaxf(col.tlv, T_L_MIN), tlw = fmaxf(col.tlw, T_L_MIN);
-
-            const float dsig2 = (sw_hi * sw_hi - sw_lo * sw_lo) / fmaxf(z_hi - z_lo, 1.0f);
-            const float sw_sq = fmaxf(sw * sw, SIGMA_MIN * SIGMA_MIN);
-
-            // --- density drift (hanna.py:993-1006)
-            const float rho_c = fmaxf(rho_p, 1e-3f);
-            const float drift_fwd = (sw_sq * drho_p) / rho_c;
-            const float half_bwd = -0.5f * dsig2;
-            const float dens_bwd = -drift_fwd;
-
-            // --- substep count (hanna.py:1162-1186)
-            const float kq = ceilf(delta / (p.substep_c * fmaxf(tlw, 1e-3f)));
-            int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
-            if (!(kq == kq)) k = 1;  // NaN
-            const float sub_dt = delta / (float)k;
-            // work class of this step (glide_step_args.work_key): the closure branch, whether
-            // the free-troposphere override applies, the substep count
-            last_k = 1 + (min(k, 6) - 1) + 6 * ((z_eval > S.blh ? 1 : 0) + 2 * col.branch);
-
-            // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
-            const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
-            const float umax = 4.0f * su, vmax = 4.0f * sv, wmax = 4.0f * sw;
-            const float au = ou_decay(sub_dt, tlu), av = ou_decay(sub_dt, tlv), aw = ou_decay(sub_dt, tlw);
-            const float ru = ou_amplitude(su2, au), rv = ou_amplitude(sv2, av), rw = ou_amplitude(sw2, aw);
-            const int64_t nn = p.n;
-            StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
-            for (int it = 0; it < k; ++it) {
-                float eu, ev, ew;
-                if (GENERAL && p.noise_sub) {
-                    const float* b = p.noise_sub + ((int64_t)(j * ms + it) * 3) * nn + i;
-                    eu = __ldg(b);
-                    ev = __ldg(b + nn);
-                    ew = __ldg(b + 2 * nn);
-                } else {
-                    eu = rng.next();
-                    ev = rng.next();
-                    ew = rng.next();
+                // --- column turbulence at z_eval (hanna.py:976-982)
+                Sig6 col = bl_profile(z_eval, S, sl, p.floors, sw_col);
+                if (z_eval > S.blh) {
+                    col.su = ft_sw; col.sv = ft_sw; col.sw = ft_sw;
+                    col.tlu = ft_tl; col.tlv = ft_tl; col.tlw = ft_tl;
                 }
-                const float factor = 1.0f + (wp * wp) / sw_sq;
-                const float drift_w = factor * half_bwd + dens_bwd;
-                float un = ou_step(up, au, 0.0f * sub_dt, ru, eu);
-                float vn = ou_step(vp, av, 0.0f * sub_dt, rv, ev);
-                float wn = ou_step(wp, aw, drift_w * sub_dt, rw, ew);
-                wn = fminf(fmaxf(wn, -wmax), wmax);
-                un = fminf(fmaxf(un, -umax), umax);
-                vn = fminf(fmaxf(vn, -vmax), vmax);
-                z = displace_z(z, wn, sub_dt, -1.0f);
-                lon = displace_lon(lon, un, sub_dt, -1.0f, m_per_deg_lon(lat));
-                lat = displace_lat(lat, vn, sub_dt, -1.0f);
-                reflect_surface(z, wn, 0.0f);
-                up = un; vp = vn; wp = wn;
-            }
+                const float su = fmaxf(col.su, SIGMA_MIN), sv = fmaxf(col.sv, SIGMA_MIN), sw = fmaxf(col.sw, SIGMA_MIN);
+                const float tlu = fmaxf(col.tlu, T_L_MIN), tlv = fmaxf(col.tlv, T_L_MIN), tlw = fmaxf(col.tlw, T_L_MIN);
 
-            // --- meander (hanna.py:1028-1054)
-            if (p.meander) {
-                float e0, e1;
-                if (GENERAL && p.noise_mea) {
-                    const float* b = p.noise_mea + ((int64_t)j * 2) * nn + i;
-                    e0 = __ldg(b);
-                    e1 = __ldg(b + nn);
-                } else {
-                    e0 = rng.next();
-                    e1 = rng.next();
+                const float dsig2 = (sw_hi * sw_hi - sw_lo * sw_lo) / fmaxf(z_hi - z_lo, 1.0f);
+                const float sw_sq = fmaxf(sw * sw, SIGMA_MIN * SIGMA_MIN);
+
+                // --- density drift (hanna.py:993-1006)
+                const float rho_c = fmaxf(rho_p, 1e-3f);
+                const float drift_fwd = (sw_sq * drho_p) / rho_c;
+                const float half_bwd = -0.5f * dsig2;
+                const float dens_bwd = -drift_fwd;
+
+                // --- substep count (hanna.py:1162-1186)
+                const float kq = ceilf(delta / (p.substep_c * fmaxf(tlw, 1e-3f)));
+                int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
+                if (!(kq == kq)) k = 1;  // NaN
+                const float sub_dt = delta / (float)k;
+                // work class of this step (glide_step_args.work_key): the closure branch, whether
+                // the free-troposphere override applies, the substep count
+                last_k = 1 + (min(k, 6) - 1) + 6 * ((z_eval > S.blh ? 1 : 0) + 2 * col.branch);
+
+                // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
+                const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
+                const float umax = 4.0f * su, vmax = 4.0f * sv, wmax = 4.0f * sw;
+                const float au = ou_decay(sub_dt, tlu), av = ou_decay(sub_dt, tlv), aw = ou_decay(sub_dt, tlw);
+                const float ru = ou_amplitude(su2, au), rv = ou_amplitude(sv2, av), rw = ou_amplitude(sw2, aw);
+                const int64_t nn = p.n;
+                StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
+                for (int it = 0; it < k; ++it) {
+                    float eu, ev, ew;
+                    if (GENERAL && p.noise_sub) {
+                        const float* b = p.noise_sub + ((int64_t)(j * ms + it) * 3) * nn + i;
+                        eu = __ldg(b);
+                        ev = __ldg(b + nn);
+                        ew = __ldg(b + 2 * nn);
+                    } else {
+                        eu = rng.next();
+                        ev = rng.next();
+                        ew = rng.next();
+                    }
+                    const float factor = 1.0f + (wp * wp) / sw_sq;
+                    const float drift_w = factor * half_bwd + dens_bwd;
+                    float un = ou_step(up, au, 0.0f * sub_dt, ru, eu);
+                    float vn = ou_step(vp, av, 0.0f * sub_dt, rv, ev);
+                    float wn = ou_step(wp, aw, drift_w * sub_dt, rw, ew);
+                    wn = fminf(fmaxf(wn, -wmax), wmax);
+                    un = fminf(fmaxf(un, -umax), umax);
+                    vn = fminf(fmaxf(vn, -vmax), vmax);
+                    z = displace_z(z, wn, sub_dt, -1.0f);
+                    lon = displace_lon(lon, un, sub_dt, -1.0f, m_per_deg_lon(lat));
+                    lat = displace_lat(lat, vn, sub_dt, -1.0f);
+                    reflect_surface(z, wn, 0.0f);
+                    up = un; vp = vn; wp = wn;
                 }
-                const float am = ou_decay(delta, p.meander_T);
-                const float umn = ou_step(um, am, 0.0f * delta, ou_amplitude(m_su * m_su, am), e0);
-                const float vmn = ou_step(vm, am, 0.0f * delta, ou_amplitude(m_sv * m_sv, am), e1);
-                lon = displace_lon(lon, umn, delta, -1.0f, m_per_deg_lon(lat));
-                lat = displace_lat(lat, vmn, delta, -1.0f);
-                um = umn; vm = vmn;
-            }
-            nonfinite |= !(isfinite(lon) && isfinite(lat) && isfinite(z) && isfinite(up) && isfinite(vp) &&
-                           isfinite(wp));
-        }
 
-        // --- the window's convection, fused: after the physics of its first step, before
-        // that step's footprint and escape kill (main.py:1446-1458, emanuel.py:772-805)
-        if (p.conv_column && j == p.conv_step) {
-            bool moved = false;
-            if (active) {
-                double u1, u2;
-                if (GENERAL && p.conv_uniforms) {
-                    u1 = (double)p.conv_uniforms[i];
-                    u2 = (double)p.conv_uniforms[p.n + i];
-                } else {
-                    convection_uniforms(i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi, u1, u2);
+                // --- meander (hanna.py:1028-1054)
+                if (p.meander) {
+                    float e0, e1;
+                    if (GENERAL && p.noise_mea) {
+                        const float* b = p.noise_mea + ((int64_t)j * 2) * nn + i;
+                        e0 = __ldg(b);
+                        e1 = __ldg(b + nn);
+                    } else {
+                        e0 = rng.next();
+                        e1 = rng.next();
+                    }
+                    const float am = ou_decay(delta, p.meander_T);
+                    const float umn = ou_step(um, am, 0.0f * delta, ou_amplitude(m_su * m_su, am), e0);
+                    const float vmn = ou_step(vm, am, 0.0f * delta, ou_amplitude(m_sv * m_sv, am), e1);
+                    lon = displace_lon(lon, umn, delta, -1.0f, m_per_deg_lon(lat));
+                    lat = displace_lat(lat, vmn, delta, -1.0f);
+                    um = umn; vm = vmn;
                 }
-                moved = convect_particle(p.conv_column, p.conv_nz, z, u1, u2);
+                nonfinite |= !(isfinite(lon) && isfinite(lat) && isfinite(z) && isfinite(up) && isfinite(vp) &&
+                               isfinite(wp));
             }
-            const int n_mv = __popc(__ballot_sync(0xffffffffu, moved));
-            if (p.conv_moved && lane == 0 && n_mv) atomicAdd(p.conv_moved, n_mv);
-        }
 
-        if (j >= p.post_begin) {
-            // --- time-ago bin (main.py:1459-1465) and footprint (footprint_gridder.py:154-197)
-            bool valid = false;
-            int64_t flat = -1;
-            if (active && p.fp) {
-                const float el = fmaxf(wend - sc.cursor_off, 0.0f);
-                int tb = (int)floorf(el / 3600.0f);
-                if (p.fp_T == 1) tb = min(tb, 0);
-                const float xf = floorf(((lon - p.fp_lon0) / p.fp_lon_span) * (float)p.fp_X);
-                const float yf = floorf(((lat - p.fp_lat0) / p.fp_lat_span) * (float)p.fp_Y);
-                int zb = 0;
+            // --- the window's convection, fused: after the physics of its first step, before
+            // that step's footprint and escape kill (main.py:1446-1458, emanuel.py:772-805)
+            if (p.conv_column && j == p.conv_step) {
+                bool moved = false;
+                if (active) {
+                    double u1, u2;
+                    if (GENERAL && p.conv_uniforms) {
+                        u1 = (double)p.conv_uniforms[i];
+                        u2 = (double)p.conv_uniforms[p.n + i];
+                    } else {
+                        convection_uniforms(i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi, u1, u2);
+                    }
+                    moved = convect_particle(p.conv_column, p.conv_nz, z, u1, u2);
+                }
+                const int n_mv = __popc(__ballot_sync(0xffffffffu, moved));
+                if (p.conv_moved && lane == 0 && n_mv) atomicAdd(p.conv_moved, n_mv);
+            }
+
+            if (j >= p.post_begin) {
+                // --- time-ago bin (main.py:1459-1465) and footprint (footprint_gridder.py:154-197)
+                bool valid = false;
+                int64_t flat = -1;
+                if (active && p.fp) {
+                    const float el = fmaxf(wend - sc.cursor_off, 0.0f);
+                    int tb = (int)floorf(el / 3600.0f);
+                    if (p.fp_T == 1) tb = min(tb, 0);
+                    const float xf = floorf(((lon - p.fp_lon0) / p.fp_lon_span) * (float)p.fp_X);
+                    const float yf = floorf(((lat - p.fp_lat0) / p.fp_lat_span) * (float)p.fp_Y);
+                    int zb = 0;
 #pragma unroll 1
-                for (int e = 0; e <= p.fp_Z; ++e) zb += (__ldg(p.fp_edges + e) < z) ? 1 : 0;
-                zb -= 1;
-                valid = (rid >= 0) && (rid < p.fp_R) && (xf >= 0.0f) && (xf < (float)p.fp_X) && (yf >= 0.0f) &&
-                        (yf < (float)p.fp_Y) && (zb >= 0) && (zb < p.fp_Z) && (tb >= 0) && (tb < p.fp_T);
-                if (valid) {
-                    const int slot = p.fp_ring > 0 ? tb % p.fp_ring : tb;
-                    const int n_slot = p.fp_ring > 0 ? p.fp_ring : p.fp_T;
-                    flat = ((((int64_t)rid * n_slot + slot) * p.fp_Z + zb) * p.fp_Y + (int64_t)yf) * p.fp_X +
-                           (int64_t)xf;
+                    for (int e = 0; e <= p.fp_Z; ++e) zb += (__ldg(p.fp_edges + e) < z) ? 1 : 0;
+                    zb -= 1;
+                    valid = (rid >= 0) && (rid < p.fp_R) && (xf >= 0.0f) && (xf < (float)p.fp_X) && (yf >= 0.0f) &&
+                            (yf < (float)p.fp_Y) && (zb >= 0) && (zb < p.fp_Z) && (tb >= 0) && (tb < p.fp_T);
+                    if (valid) {
+                        const int slot = p.fp_ring > 0 ? tb % p.fp_ring : tb;
+                        const int n_slot = p.fp_ring > 0 ? p.fp_ring : p.fp_T;
+                        flat = ((((int64_t)rid * n_slot + slot) * p.fp_Z + zb) * p.fp_Y + (int64_t)yf) * p.fp_X +
+                               (int64_t)xf;
+                    }
+                }
+                // weight * dt: a float32 product (the float32 gridder's w_eff) or an FP64 one
+                const double w_dt = p.fp64 ? (double)wgt * (double)sc.delta : (double)(wgt * sc.delta);
+                if (valid && flat == fp_cell) {
+                    fp_acc += w_dt;
+                } else {
+                    if (fp_cell >= 0) footprint_flush(p, fp_cell, fp_acc);
+                    fp_cell = valid ? flat : -1;
+                    fp_acc = valid ? w_dt : 0.0;
+                }
+                // --- escape kill (main.py:690-711, 1475-1477)
+                bool escaped = false;
+                if (active) {
+                    const bool within = (lon >= p.dom_lon0) && (lon <= p.dom_lon1) && (lat >= p.dom_lat0) &&
+                                        (lat <= p.dom_lat1) && (z <= p.dom_alt);
+                    escaped = !within;
+                    if (escaped) alive = false;
+                }
+                const int n_esc = __popc(__ballot_sync(0xffffffffu, escaped));
+                const int n_act = __popc(__ballot_sync(0xffffffffu, active));
+                if (lane == 0) {
+                    if (n_esc) atomicAdd(&s_counts[j], n_esc);
+                    if (n_act) atomicAdd(&s_counts[p.n_steps + j], n_act);
+                }
+                // --- mean-position diagnostic (main.py:1565-1566): sums over every particle
+                if (p.diag) {
+                    const double sx = warp_sum(have ? (double)lon : 0.0);
+                    const double sy = warp_sum(have ? (double)lat : 0.0);
+                    const double sz = warp_sum(have ? (double)z : 0.0);
+                    if (lane == 0) {
+                        atomicAdd(&s_diag[3 * j], sx);
+                        atomicAdd(&s_diag[3 * j + 1], sy);
+                        atomicAdd(&s_diag[3 * j + 2], sz);
+                    }
                 }
             }
-            if (valid && flat == fp_cell) {
-                fp_acc += wgt * sc.delta;
-            } else {
-                if (fp_cell >= 0) atomicAdd(p.fp + fp_cell, fp_acc);
-                fp_cell = valid ? flat : -1;
-                fp_acc = valid ? wgt * sc.delta : 0.0f;
-            }
-            // --- escape kill (main.py:690-711, 1475-1477)
-            bool escaped = false;
-            if (active) {
-                const bool within = (lon >= p.dom_lon0) && (lon <= p.dom_lon1) && (lat >= p.dom_lat0) &&
-                                    (lat <= p.dom_lat1) && (z <= p.dom_alt);
-                escaped = !within;
-                if (escaped) alive = false;
-            }
-            const int n_esc = __popc(__ballot_sync(0xffffffffu, escaped));
-            const int n_act = __popc(__ballot_sync(0xffffffffu, active));
-            if (lane == 0) {
-                if (n_esc) atomicAdd(&s_counts[j], n_esc);
-                if (n_act) atomicAdd(&s_counts[p.n_steps + j], n_act);
-            }
         }
-    }
 
-    if (fp_cell >= 0) atomicAdd(p.fp + fp_cell, fp_acc);
-    if (have) {
-        p.lon[i * p.ps] = lon;
-        p.lat[i * p.ps] = lat;
-        p.z[i * p.ps] = z;
-        p.up[i] = up;
-        p.vp[i] = vp;
-        p.wp[i] = wp;
-        if (p.meander) { p.um[i] = um; p.vm[i] = vm; }
-        if (p.alive) p.alive[i] = alive ? 1 : 0;
-        if (nonfinite && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_NONFINITE_STATE);
-        if (p.work_key) {
-            int key = GLIDE_WORK_DONE;
-            if (alive) {
-                const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
-                if (!(GENERAL && p.active_mask) && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
-                else if (last_active) key = last_k;
+        if (fp_cell >= 0) footprint_flush(p, fp_cell, fp_acc);
+        if (have) {
+            p.lon[i * p.ps] = lon;
+            p.lat[i * p.ps] = lat;
+            p.z[i * p.ps] = z;
+            p.up[i] = up;
+            p.vp[i] = vp;
+            p.wp[i] = wp;
+            if (p.meander) { p.um[i] = um; p.vm[i] = vm; }
+            if (p.alive) p.alive[i] = alive ? 1 : 0;
+            if (nonfinite && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_NONFINITE_STATE);
+            if (p.work_key) {
+                int key = GLIDE_WORK_DONE;
+                if (alive) {
+                    const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
+                    if (!(GENERAL && p.active_mask) && !(rel >= sl.cursor_off)) key = GLIDE_WORK_PENDING;
+                    else if (last_active) key = last_k;
+                }
+                p.work_key[i] = (uint8_t)key;
             }
-            p.work_key[i] = (uint8_t)key;
         }
     }
     if (bad_order && p.status) atomicOr(p.status, (uint32_t)GLIDE_STATUS_BAD_ORDER);
@@ -596,6 +686,9 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
         if (p.esc && s_counts[k]) atomicAdd(p.esc + k, s_counts[k]);
         if (p.act && s_counts[p.n_steps + k]) atomicAdd(p.act + k, s_counts[p.n_steps + k]);
     }
+    if (p.diag)
+        for (int k = threadIdx.x + p.post_begin * 3; k < 3 * p.n_steps; k += blockDim.x)
+            atomicAdd(p.diag + k, s_diag[k] + s_static[k % 3]);
 }
 
 template <typename T, int THREADS, int MIN_BLOCKS, bool GENERAL>
@@ -630,8 +723,10 @@ static void launch_shape(const StepDev& d, cudaStream_t stream, size_t smem) {
 
 template <typename T>
 static glide_status launch_step(const StepDev& d, cudaStream_t stream, int variant) {
-    const size_t smem = sizeof(int32_t) * 2 * (size_t)d.n_steps;
-    if (smem > 48 * 1024) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large", d.n_steps);
+    const size_t smem = step_smem_bytes(d.n_steps, d.diag != nullptr);
+    if (smem > 48 * 1024)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large%s", d.n_steps,
+                         d.diag ? " with diag_pos_sum (at most 1535)" : "");
     switch (variant) {
         case 0: launch_shape<T, 0, false>(d, stream, smem); break;
         case 1: launch_shape<T, 1, false>(d, stream, smem); break;
@@ -668,6 +763,12 @@ static glide_status validate_step(const glide_step_args* a) {
     if (a->grid.nz < 2 || a->grid.ny < 2 || a->grid.nx < 2)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: grid must be at least 2x2x2");
     if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
+    if (a->phys_begin < 0 || a->post_begin < 0)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: phys_begin / post_begin < 0");
+    if (a->diag_pos_sum && ((uintptr_t)a->diag_pos_sum & 7u))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: diag_pos_sum must be 8-byte aligned");
+    if (a->footprint && a->fp.value_f64 && ((uintptr_t)a->footprint & 7u))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: a float64 footprint must be 8-byte aligned");
     if (a->launch_variant < 0 || a->launch_variant >= kNumVariants)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", a->launch_variant);
     if (a->pos_stride < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: pos_stride < 1");
@@ -707,6 +808,7 @@ static StepDev make_step_dev(const glide_step_args* a) {
     d.noise_sub = a->noise_substep; d.noise_mea = a->noise_meander;
     d.seed_lo = (uint32_t)a->seed; d.seed_hi = (uint32_t)(a->seed >> 32);
     d.fp = a->footprint;
+    d.fp64 = a->fp.value_f64 != 0;
     d.fp_lon0 = (float)a->fp.lon_min;
     d.fp_lon_span = (float)fmax(1e-6, a->fp.lon_max - a->fp.lon_min);
     d.fp_lat0 = (float)a->fp.lat_min;
@@ -722,6 +824,7 @@ static StepDev make_step_dev(const glide_step_args* a) {
     d.order = a->order; d.work_key = a->work_key;
     d.conv_column = static_cast<const double*>(a->conv_column); d.conv_step = a->conv_step; d.conv_nz = a->conv_nz;
     d.conv_uniforms = a->conv_uniforms; d.conv_moved = a->conv_moved;
+    d.diag = a->diag_pos_sum;
     return d;
 }
 
@@ -759,6 +862,7 @@ extern "C" glide_status glide_step_batched(const glide_step_args* args, int32_t 
     bool general = false;
     int32_t dtype = -1;
     int max_steps = 1;
+    bool diag = false;
     uint64_t blocks = 0;
     for (int k = 0; k < count; ++k) {
         const glide_step_args* a = args + k;
@@ -770,6 +874,7 @@ extern "C" glide_status glide_step_batched(const glide_step_args* args, int32_t 
         const StepDev d = make_step_dev(a);
         general = general || needs_general(d);
         max_steps = max(max_steps, d.n_steps);
+        diag = diag || d.diag != nullptr;
         b.d[b.count] = d;
         b.block_start[b.count] = (uint32_t)blocks;
         blocks += (uint64_t)((d.n + 127) / 128);
@@ -778,7 +883,9 @@ extern "C" glide_status glide_step_batched(const glide_step_args* args, int32_t 
     if (b.count == 0) return GLIDE_OK;
     if (blocks > 0x7fffffffull) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: too many particles");
     b.block_start[b.count] = (uint32_t)blocks;
-    const size_t smem = sizeof(int32_t) * 2 * (size_t)max_steps;
+    // every block lays out shared memory for the longest batch (and the diagnostic sums
+    // when any batch asks for them); a block uses the part its own batch needs
+    const size_t smem = step_smem_bytes(max_steps, diag);
     if (smem > 48 * 1024)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step_batched: n_steps %d too large", max_steps);
     cudaStream_t s = (cudaStream_t)stream;

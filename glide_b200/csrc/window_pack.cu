@@ -46,7 +46,40 @@ struct PackDev {
     const float* h3; const float* hlev; const float* p_hpa;
     float meander_coeff; int radius; int build_meander;
     void* wind; void* surf; void* support;
+    double* wind_sum;
 };
+
+// Sums of u, v, w of both snapshots over every cell (the grid means of the per-step
+// wind diagnostic, main.py:892-938): a grid-stride loop, warp and block reductions in
+// FP64, one atomic per block and channel.
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) wind_sum_kernel(const PackDev d) {
+    __shared__ double s_part[kSumThreads / 32][6];
+    const int64_t ncell = (int64_t)d.nz * d.ny * d.nx;
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+        acc[0] += __ldg(d.u[0] + c);
+        acc[1] += __ldg(d.v[0] + c);
+        acc[2] += __ldg(d.w[0] + c);
+        acc[3] += __ldg(d.u[1] + c);
+        acc[4] += __ldg(d.v[1] + c);
+        acc[5] += __ldg(d.w[1] + c);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_part[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int w = 0; w < kSumThreads / 32; ++w) v += s_part[w][threadIdx.x];
+        atomicAdd(d.wind_sum + threadIdx.x, v);
+    }
+}
 
 template <typename T>
 __global__ void pack_surf_kernel(const PackDev d) {
@@ -202,6 +235,7 @@ static glide_status launch_pack(const PackDev& d, cudaStream_t s) {
     const bool tiled = d.build_meander && d.radius <= kMaxTileRadius;
     const size_t smem = tiled ? sizeof(float) * 2 * (size_t)(kTileX + 2 * d.radius) * (kTileY + 2 * d.radius) : 0;
     pack_cells_kernel<T><<<grid, dim3(kTileX, kTileY), smem, s>>>(d);
+    if (d.wind_sum) wind_sum_kernel<<<148 * 2, kSumThreads, 0, s>>>(d);
     return check_launch("glide_window_pack");
 }
 
@@ -237,6 +271,8 @@ extern "C" glide_status glide_window_pack(const glide_window_desc* w, void* stre
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_window_pack: an output brick is NULL");
     if (((uintptr_t)w->wind_packed | (uintptr_t)w->surf_packed | (uintptr_t)w->support_packed) & 15u)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_window_pack: output bricks must be 16-byte aligned");
+    if ((uintptr_t)w->wind_sum & 7u)
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_window_pack: wind_sum must be 8-byte aligned");
     if (w->build_meander && w->meander_radius < 1)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_window_pack: meander_radius must be >= 1");
     if (g.nz > 65535 || (g.ny + kTileY - 1) / kTileY > 65535)
@@ -250,6 +286,7 @@ extern "C" glide_status glide_window_pack(const glide_window_desc* w, void* stre
     d.h3 = w->height3d; d.hlev = w->height_level; d.p_hpa = w->pressure_hpa;
     d.meander_coeff = w->meander_coefficient; d.radius = w->meander_radius; d.build_meander = w->build_meander;
     d.wind = w->wind_packed; d.surf = w->surf_packed; d.support = w->support_packed;
+    d.wind_sum = w->wind_sum;
     cudaStream_t s = (cudaStream_t)stream;
     switch (w->met_dtype) {
         case GLIDE_MET_F32: return launch_pack<float>(d, s);

@@ -33,64 +33,8 @@ import numpy as np
 import torch
 
 from glide_b200 import _abi
+from glide_b200.config import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig  # noqa: F401 (re-exported)
 from glide_b200.window import GridInfo, PackedWindow, WindowFields, stream_handle
-
-
-@dataclass(frozen=True)
-class HannaConfig:
-    """``HannaScheme`` knobs (src/lpdm/turbulence/hanna.py:440-520)."""
-
-    meander_enabled: bool = False
-    meander_coefficient: float = 0.16
-    meander_stencil_radius: int = 1
-    meander_timescale_seconds: float = 1800.0
-    substep_c: float = 0.5
-    max_substeps: int = 50
-    z_ubl_m: float = 2.0
-    flexpart_tl_floors: bool = True
-    surface_layer_override: bool = False
-
-
-@dataclass(frozen=True)
-class EmanuelConfig:
-    """``EmanuelReducedConvection`` knobs (src/lpdm/convection/emanuel.py:531-565)."""
-
-    closure_c: float = 0.03
-    trigger_dtv_k: float = 0.9
-    min_cape_j_kg: float = 50.0
-    min_cloud_depth_m: float = 500.0
-
-
-@dataclass(frozen=True)
-class FootprintSpec:
-    """``OutputGridConfig`` and the gridder's release count (src/lpdm/config.py:360-382)."""
-
-    lon_bounds: tuple[float, float]
-    lat_bounds: tuple[float, float]
-    n_x: int
-    n_y: int
-    z_edges: tuple[float, ...]
-    n_time_bins: int
-    n_releases: int = 1
-    ring: int = 0  # > 0: keep only `ring` live time-ago slices per release, flushed as bins complete
-
-    @property
-    def shape(self) -> tuple[int, int, int, int, int]:
-        return (self.n_releases, self.n_time_bins, len(self.z_edges) - 1, self.n_y, self.n_x)
-
-    @property
-    def device_shape(self) -> tuple[int, int, int, int, int]:
-        t = self.ring if self.ring > 0 else self.n_time_bins
-        return (self.n_releases, t, len(self.z_edges) - 1, self.n_y, self.n_x)
-
-
-@dataclass(frozen=True)
-class DomainSpec:
-    """``MetDomainConfig`` bounds of the escape kill (src/lpdm/main.py:690-711)."""
-
-    lon_bounds: tuple[float, float]
-    lat_bounds: tuple[float, float]
-    alt_max_m: float
 
 
 @dataclass
@@ -283,6 +227,25 @@ class BatchOutput:
     n_steps: int
     convection: list = field(default_factory=list)  # (window start, n_moved device tensor)
     status: int = 0
+    # per-step diagnostics of the reference runtime (main.py:1565-1566, 1612-1643), float32
+    # [n_steps, 3]: mean (lon, lat, z) of all particles after the step, and the grid-mean
+    # (u, v, w) of the step's window lerped by its RK2 weight; None when not computed
+    diag_pos: np.ndarray | None = None
+    diag_wind: np.ndarray | None = None
+
+    def diagnostic_rows(self) -> list[dict]:
+        """The per-step rows the reference's runtime writes (main.py:1612-1643) for this
+        batch: step number within the batch, mean position, mean wind, active, escaped and
+        alive counts."""
+        if self.diag_pos is None:
+            raise ValueError("the batch ran without diagnostics")
+        n = int(self.state.n)
+        alive = n - np.cumsum(self.escaped_per_step)
+        return [{"step": k + 1, "mean_lon": float(p[0]), "mean_lat": float(p[1]), "mean_alt_agl_m": float(p[2]),
+                 "u_mean_m_s": float(w[0]), "v_mean_m_s": float(w[1]), "w_mean_m_s": float(w[2]),
+                 "active_particles": int(a), "escaped_this_step": int(e), "alive_particles": int(al)}
+                for k, (p, w, a, e, al) in enumerate(zip(self.diag_pos, self.diag_wind, self.active_per_step,
+                                                         self.escaped_per_step, alive))]
 
 
 class BatchRun:
@@ -298,8 +261,13 @@ class BatchRun:
         self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        # per-step diagnostics: position sums [n_steps][3] (the step kernel adds to them) and
+        # each window's wind sums [n_windows][6] (copied from its packed window)
+        self.diagnostics = runner.diagnostics
+        self.diag_sum = torch.zeros((max(1, len(steps)), 3), dtype=torch.float64, device=dev) \
+            if self.diagnostics else None
         fp = runner.footprint
-        self.footprint = torch.zeros(fp.device_shape, dtype=torch.float32, device=dev)
+        self.footprint = torch.zeros(fp.device_shape, dtype=fp.torch_dtype, device=dev)
         self.footprint_out = None
         self.sink = runner.footprint_sink
         if fp.ring > 0:
@@ -317,7 +285,7 @@ class BatchRun:
                     ends[r] = vals[0]
             self.release_end = ends
             if self.sink is None:
-                self.footprint_out = torch.zeros(fp.shape, dtype=torch.float32, device=dev)
+                self.footprint_out = torch.zeros(fp.shape, dtype=fp.torch_dtype, device=dev)
                 out = self.footprint_out
 
                 rows_out = out.view(fp.n_releases * fp.n_time_bins, -1)
@@ -329,6 +297,8 @@ class BatchRun:
         self.z_edges = _upload(torch.as_tensor(np.asarray(runner.footprint.z_edges, dtype=np.float32)), dev)
         # windows = runs of consecutive steps with the same hour
         self.windows: list[tuple[int, int]] = window_ranges(steps)
+        self.wind_sum = torch.zeros((max(1, len(self.windows)), 6), dtype=torch.float64, device=dev) \
+            if self.diagnostics else None
         self.next_window = 0
         self.conv_log: list = []
         # per-window preparation, double-buffered when pipelined (bricks and column of
@@ -392,7 +362,7 @@ class BatchRun:
         fp = r.footprint
         a.fp = _abi.FootprintGrid(fp.lon_bounds[0], fp.lon_bounds[1], fp.lat_bounds[0], fp.lat_bounds[1],
                                   fp.n_releases, fp.n_time_bins, len(fp.z_edges) - 1, fp.n_y, fp.n_x,
-                                  self.z_edges.data_ptr(), fp.ring)
+                                  self.z_edges.data_ptr(), fp.ring, 1 if fp.value_dtype == "f64" else 0)
         d = r.domain
         a.dom_lon_min, a.dom_lon_max = d.lon_bounds
         a.dom_lat_min, a.dom_lat_max = d.lat_bounds
@@ -400,6 +370,7 @@ class BatchRun:
         a.escaped_per_step = self.esc.data_ptr() + 4 * j0
         a.active_per_step = self.act.data_ptr() + 4 * j0
         a.status = self.status.data_ptr()
+        a.diag_pos_sum = None if self.diag_sum is None else self.diag_sum.data_ptr() + 24 * j0
         a.launch_variant = r.launch_variant
         if self.work_key is not None:
             a.order = self.order.data_ptr() if self.order_valid else None
@@ -456,6 +427,7 @@ class BatchRun:
         self.next_window += 1
         first = self.steps[j0]
         packed = r.packed_provider(first.hour)
+        self._record_wind_sum(k, packed, stream)
         noise = self._noise(j0, j1)
         keep = [packed, noise]
         a = self._step_args(packed, j0, j1 - j0, 0, 0, noise)
@@ -468,6 +440,16 @@ class BatchRun:
             a.conv_uniforms, a.conv_moved = conv["conv_uniforms"], conv["conv_moved"]
             keep += [col, conv["keep"]]
         return a, keep
+
+    def _record_wind_sum(self, k: int, packed: PackedWindow, stream) -> None:
+        """Window k's wind sums (computed when its bricks were packed) into the batch's
+        per-window table, on ``stream`` after the packing."""
+        if self.wind_sum is None:
+            return
+        if packed.wind_sum is None:
+            raise ValueError("diagnostics need packed windows with wind sums (PackedWindow.pack)")
+        with torch.cuda.stream(stream):
+            self.wind_sum[k].copy_(packed.wind_sum, non_blocking=True)
 
     def _reorder(self, sh) -> None:
         """Rebuild the particle order from the work keys of the last launch."""
@@ -557,6 +539,7 @@ class BatchRun:
             self._prepare(k)
         wf, packed, scratch, ready = self.prepared.pop(k)
         main.wait_event(ready)
+        self._record_wind_sum(k, packed, main)
         noise = self._noise(j0, j1)
         if main is not caller:  # the caller's work so far (state, noise) comes first
             main.wait_stream(caller)
@@ -703,8 +686,26 @@ class BatchRun:
         n = len(self.steps)
         status = int(self.status.item())
         fp = self.footprint if self.r.footprint.ring == 0 else self.footprint_out
-        return BatchOutput(self.state, fp, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
-                           self.conv_log, status)
+        out = BatchOutput(self.state, fp, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
+                          self.conv_log, status)
+        if self.diag_sum is not None and n > 0:
+            out.diag_pos = (self.diag_sum[:n].cpu().numpy() / max(1, self.state.n)).astype(np.float32)
+            out.diag_wind = self._diag_wind(self.wind_sum.cpu().numpy())
+        return out
+
+    def _diag_wind(self, sums: np.ndarray) -> np.ndarray:
+        """Per-step grid-mean wind from the windows' sums: the float32 means of the two
+        snapshots lerped by the step's RK2 weight as _advection_alpha_wind_mean does
+        (main.py:892-938: ``mean_start * (1 - alpha) + mean_end * alpha`` in float32)."""
+        ncell = float(np.prod(self.r.grid.shape))
+        out = np.zeros((len(self.steps), 3), dtype=np.float32)
+        for k, (j0, j1) in enumerate(self.windows):
+            m0 = (sums[k, :3] / ncell).astype(np.float32)
+            m1 = (sums[k, 3:] / ncell).astype(np.float32)
+            alpha = np.asarray([self.steps[j].alpha for j in range(j0, j1)], dtype=np.float64)
+            om = (1.0 - alpha).astype(np.float32)[:, None]
+            out[j0:j1] = m0[None, :] * om + m1[None, :] * alpha.astype(np.float32)[:, None]
+        return out
 
 
 def launch_grouped(args: list, stream) -> None:
@@ -725,11 +726,13 @@ class HostSliceStream:
     indices into one of ``buffers`` alternating pinned buffers; ``on_host(r_idx,
     b_idx, slices)`` (int64 numpy arrays and a pinned CPU tensor ``[k, Zb, Y, X]``,
     valid during the call) runs on the host once a copy has landed: when its buffer
-    is needed again, or at ``drain()``. ``bytes_moved`` counts the slice bytes."""
+    is needed again, or at ``drain()``. ``bytes_moved`` counts the slice bytes.
+    ``dtype`` is the footprint's value type (float32 or float64)."""
 
     def __init__(self, device, slice_shape: tuple, capacity: int, on_host: Callable | None = None,
-                 buffers: int = 2) -> None:
+                 buffers: int = 2, dtype: torch.dtype = torch.float32) -> None:
         self.device = torch.device(device)
+        self.dtype = dtype
         self.slice_shape = tuple(slice_shape)
         self.on_host = on_host
         self.copy_stream = torch.cuda.Stream(device=self.device)
@@ -739,7 +742,7 @@ class HostSliceStream:
         self.bytes_moved = 0
 
     def _alloc(self, k: int) -> dict:
-        return {"slices": torch.empty((k,) + self.slice_shape, dtype=torch.float32).pin_memory(),
+        return {"slices": torch.empty((k,) + self.slice_shape, dtype=self.dtype).pin_memory(),
                 "idx": torch.empty((2, k), dtype=torch.int64).pin_memory()}
 
     def _deliver(self, slot: int) -> None:
@@ -817,6 +820,7 @@ class BatchRunner:
         self.steps_per_launch: int | None = None  # split each window into launches of this many steps
         self.fuse_convection = True  # convection inside the step kernel (else its own kernel between two steps)
         self.column_cache: dict | None = None  # (hour, alpha) -> prebuilt convection column, shared by batches
+        self.diagnostics = True  # per-step mean position and grid-mean wind (BatchOutput.diag_pos / diag_wind)
         self._step_stream = None
         self._slots: list[PackedWindow | None] = [None, None]
 

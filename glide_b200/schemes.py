@@ -119,6 +119,17 @@ def get_convection_scheme(name: str, **kwargs) -> ConvectionScheme:
     return _CONV[name](**kwargs)
 
 
+def register_with_reference(turbulence_base, convection_base) -> None:
+    """Registers ``hanna_1982_b200`` and ``emanuel_reduced_b200`` in the reference's own
+    scheme registries, given its ``lpdm.turbulence.base`` and ``lpdm.convection.base``
+    modules (``register_scheme``, turbulence/base.py:96-107, convection/base.py:102-113),
+    so its ``get_scheme`` / ``get_convection_scheme`` build them by name and its runtime
+    (``lpdm.main._run``) runs them. The registries check only the ``name`` attribute,
+    which these classes share with their registrations here."""
+    turbulence_base.register_scheme(HannaB200Scheme)
+    convection_base.register_scheme(EmanuelB200Convection)
+
+
 def list_schemes() -> tuple[str, ...]:
     return tuple(sorted(_TURB))
 
@@ -392,15 +403,16 @@ class FootprintGridderB200:
         n_z = int(z_edges.size - 1)
         if min(n_time_bins, n_y, n_x, n_releases) <= 0 or n_z <= 0:
             raise ValueError("All footprint dimensions must be > 0")
-        if dtype != torch.float32:
-            raise ValueError("FootprintGridderB200 accumulates in float32")
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError("FootprintGridderB200 accumulates in float32 or float64")
         self.device = torch.device(device)
         self.dtype = dtype
         n_elements = int(n_releases) * int(n_time_bins) * n_z * int(n_y) * int(n_x)
         env_cap = os.environ.get("LPDM_FOOTPRINT_MAX_GIB")
         cap_gib = float(env_cap) if env_cap else self.MAX_FOOTPRINT_GIB
-        if n_elements * 4 > int(cap_gib * 1024**3):
-            raise MemoryError(f"Footprint tensor would require {n_elements * 4 / 1024**3:.2f} GiB; cap is "
+        elem = torch.empty((), dtype=dtype).element_size()
+        if n_elements * elem > int(cap_gib * 1024**3):
+            raise MemoryError(f"Footprint tensor would require {n_elements * elem / 1024**3:.2f} GiB; cap is "
                               f"{cap_gib:.2f} GiB (raise it via LPDM_FOOTPRINT_MAX_GIB)")
         self.tensor = torch.zeros((n_releases, n_time_bins, n_z, n_y, n_x), device=self.device, dtype=dtype)
         self.lon_min, self.lon_max = lon_bounds
@@ -411,7 +423,8 @@ class FootprintGridderB200:
 
     def accumulate(self, particles: torch.Tensor, active_mask: torch.Tensor, weights: torch.Tensor,
                    t_idx: torch.Tensor, release_idx: torch.Tensor, dt_seconds: float) -> None:
-        """Adds ``weights * dt_seconds`` of every active in-range particle to its cell."""
+        """Adds ``weights * dt_seconds`` of every active in-range particle to its cell
+        (formed and summed in FP64 when the gridder is float64)."""
         _require_cuda(particles, "particles")
         n = particles.shape[0]
         if particles.dim() != 2 or particles.shape[1] < 3 or particles.dtype != torch.float32:
@@ -421,7 +434,8 @@ class FootprintGridderB200:
         if weights.dim() != 1 or weights.dtype != torch.float32:
             raise ValueError("weights must be a float32 (N,) tensor")
         g = _abi.FootprintGrid(self.lon_min, self.lon_max, self.lat_min, self.lat_max, self.n_releases, self.n_t,
-                               self.n_z, self.n_y, self.n_x, self.z_edges.data_ptr())
+                               self.n_z, self.n_y, self.n_x, self.z_edges.data_ptr(), 0,
+                               1 if self.dtype == torch.float64 else 0)
         act = active_mask.to(dtype=torch.uint8).contiguous()
         t32 = t_idx.to(dtype=torch.int32).contiguous()
         r32 = release_idx.to(dtype=torch.int32).contiguous()

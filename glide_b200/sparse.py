@@ -7,7 +7,8 @@ mostly zeros (a plume covers a few thousand of the 1.1e5 cells of the EUROPE gri
 in an hour), so here the ring footprint's completed slices are compacted on the
 device (``glide_footprint_compact``) and only the non-zero cells cross PCIe:
 
-* ``compact_rows`` — one compaction of rows of a ``[n_rows, cells]`` float32 tensor;
+* ``compact_rows`` — one compaction of rows of a ``[n_rows, cells]`` float32 (or
+  float64) tensor;
 * ``SparseSliceStream`` — a ring-footprint sink (``BatchRunner(footprint_sink=...)``):
   compacts the window's completed slices on the step stream (and clears their ring
   slots), copies the lists to pinned host memory on a copy stream and hands them
@@ -16,7 +17,7 @@ device (``glide_footprint_compact``) and only the non-zero cells cross PCIe:
   gathered per release into the ``(1, T, Z, Y, X)`` regions the reference's writer
   takes (``region_writer``).
 
-A cell is kept when its float32 bit pattern is not zero, so ``densify`` rebuilds the
+A cell is kept when its value's bit pattern is not zero, so ``densify`` rebuilds the
 dense slice bit-exactly.
 """
 
@@ -44,12 +45,13 @@ def compact_rows(rows: torch.Tensor, row_index: torch.Tensor, *, clear: bool = F
                  stream: torch.cuda.Stream | None = None):
     """Compacts ``rows[row_index[s]]`` for s in [0, k) on ``stream`` (default: the current
     stream), without synchronising. Returns device tensors ``(slice_offset [k + 1] int64,
-    cell [capacity] int32, value [capacity] float32)``; slice s holds entries
+    cell [capacity] int32, value [capacity] of the rows' dtype)``; slice s holds entries
     ``[slice_offset[s], slice_offset[s + 1])``. ``capacity`` defaults to ``k * cells``
     (every cell non-zero), which cannot overflow. ``clear`` sets the compacted rows to zero.
     ``out`` reuses ``(slice_offset, cell, value)`` tensors, ``scratch`` a uint8 tensor."""
-    if rows.device.type != "cuda" or rows.dtype != torch.float32 or rows.dim() != 2 or not rows.is_contiguous():
-        raise ValueError("rows must be a contiguous 2-D float32 CUDA tensor")
+    if (rows.device.type != "cuda" or rows.dtype not in (torch.float32, torch.float64) or rows.dim() != 2
+            or not rows.is_contiguous()):
+        raise ValueError("rows must be a contiguous 2-D float32 or float64 CUDA tensor")
     if row_index.dtype != torch.int64 or row_index.device != rows.device or not row_index.is_contiguous():
         raise ValueError("row_index must be a contiguous int64 tensor on the rows' device")
     n_rows, cells = rows.shape
@@ -59,10 +61,12 @@ def compact_rows(rows: torch.Tensor, row_index: torch.Tensor, *, clear: bool = F
     if out is None:
         out = (torch.empty(k + 1, dtype=torch.int64, device=dev),
                torch.empty(max(cap, 1), dtype=torch.int32, device=dev),
-               torch.empty(max(cap, 1), dtype=torch.float32, device=dev))
+               torch.empty(max(cap, 1), dtype=rows.dtype, device=dev))
     off, cell, value = out
     if off.numel() < k + 1 or cell.numel() < cap or value.numel() < cap:
         raise ValueError("output tensors smaller than k + 1 offsets / capacity entries")
+    if value.dtype != rows.dtype:
+        raise ValueError("the value output must have the rows' dtype")
     need = _scratch_bytes(k, cells)
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(max(need, 8), dtype=torch.uint8, device=dev)
@@ -72,16 +76,17 @@ def compact_rows(rows: torch.Tensor, row_index: torch.Tensor, *, clear: bool = F
     a.slice_offset, a.out_cell, a.out_value, a.capacity = off.data_ptr(), cell.data_ptr(), value.data_ptr(), cap
     a.status = None if status is None else status.data_ptr()
     a.scratch, a.scratch_bytes = scratch.data_ptr(), scratch.numel()
+    a.value_f64 = 1 if rows.dtype == torch.float64 else 0
     _abi.check(_abi.lib.glide_footprint_compact(C.byref(a), stream_handle(stream)), "glide_footprint_compact")
     return off, cell, value
 
 
 def densify(slice_offset: np.ndarray, cell: np.ndarray, value: np.ndarray, slice_shape: tuple) -> np.ndarray:
-    """(slice_offset [k + 1], cell, value) -> dense float32 slices [k, *slice_shape]."""
+    """(slice_offset [k + 1], cell, value) -> dense slices [k, *slice_shape] of the values' dtype."""
     slice_offset = np.asarray(slice_offset, dtype=np.int64)
     k = slice_offset.size - 1
     n = int(np.prod(slice_shape))
-    out = np.zeros((k, n), dtype=np.float32)
+    out = np.zeros((k, n), dtype=np.asarray(value).dtype)
     total = int(slice_offset[-1])
     owner = np.repeat(np.arange(k), np.diff(slice_offset))
     out[owner, np.asarray(cell[:total], dtype=np.int64)] = value[:total]
@@ -104,11 +109,14 @@ class SparseSliceStream:
     front.
 
     ``bytes_moved`` counts the bytes copied to the host; ``dense_bytes`` what the dense
-    slices would have been."""
+    slices would have been. ``dtype`` is the footprint's value type (float32 or float64)."""
 
     def __init__(self, device, slice_shape: tuple, on_host: Callable | None = None, buffers: int = 2,
-                 headroom: float = 1.25, initial_density: float = 1.0 / 32.0, capacity: int = 0) -> None:
+                 headroom: float = 1.25, initial_density: float = 1.0 / 32.0, capacity: int = 0,
+                 dtype: torch.dtype = torch.float32) -> None:
         self.device = torch.device(device)
+        self.dtype = dtype
+        self.value_bytes = torch.empty((), dtype=dtype).element_size()
         self.slice_shape = tuple(int(s) for s in slice_shape)
         self.cells = int(np.prod(self.slice_shape))
         self.on_host = on_host
@@ -135,7 +143,7 @@ class SparseSliceStream:
         slot["k"] = kk
         slot["off"] = torch.empty(kk + 1, dtype=torch.int64, device=d)
         slot["cell"] = torch.empty(kk * self.cells, dtype=torch.int32, device=d)
-        slot["value"] = torch.empty(kk * self.cells, dtype=torch.float32, device=d)
+        slot["value"] = torch.empty(kk * self.cells, dtype=self.dtype, device=d)
         slot["scratch"] = torch.empty(_scratch_bytes(kk, self.cells), dtype=torch.uint8, device=d)
         slot["h_off"] = torch.empty(kk + 1, dtype=torch.int64).pin_memory()
         slot["h_idx"] = torch.empty((2, kk), dtype=torch.int64).pin_memory()
@@ -146,7 +154,7 @@ class SparseSliceStream:
         nn = max(n, 1, int(slot["h"] * 1.5) + 1)
         slot["h"] = nn
         slot["h_cell"] = torch.empty(nn, dtype=torch.int32).pin_memory()
-        slot["h_value"] = torch.empty(nn, dtype=torch.float32).pin_memory()
+        slot["h_value"] = torch.empty(nn, dtype=self.dtype).pin_memory()
 
     def _deliver(self, i: int) -> None:
         p = self.pending[i]
@@ -170,7 +178,7 @@ class SparseSliceStream:
                 slot["h_value"][spec:total].copy_(slot["value"][spec:total], non_blocking=True)
                 ev = self.copy_stream.record_event()
             ev.synchronize()
-            self.bytes_moved += (total - spec) * 8
+            self.bytes_moved += (total - spec) * (4 + self.value_bytes)
         if k > 0:
             self.per_slice = max(self.per_slice, float(np.diff(off).max()))
         self.entries += total
@@ -181,7 +189,7 @@ class SparseSliceStream:
 
     def from_rows(self, rows: torch.Tensor, flat: torch.Tensor, r_idx: torch.Tensor, b_idx: torch.Tensor,
                   clear: bool = True) -> None:
-        """Slices ``rows[flat[s]]`` ([n_rows, cells] float32, on the current stream's device)
+        """Slices ``rows[flat[s]]`` ([n_rows, cells] of the stream's dtype, on the current stream's device)
         for (release r_idx[s], bin b_idx[s]); ``clear`` zeroes those rows after reading them
         (``flat`` must then be distinct)."""
         k = int(flat.numel())
@@ -208,8 +216,8 @@ class SparseSliceStream:
                 t.record_stream(self.copy_stream)
             done = self.copy_stream.record_event()
         self.pending[i] = (done, k, spec)
-        self.bytes_moved += spec * 8 + (k + 1) * 8  # footprint data only, as HostSliceStream counts it
-        self.dense_bytes += k * self.cells * 4
+        self.bytes_moved += spec * (4 + self.value_bytes) + (k + 1) * 8  # footprint data only
+        self.dense_bytes += k * self.cells * self.value_bytes
 
     def __call__(self, r_idx: torch.Tensor, b_idx: torch.Tensor, slices: torch.Tensor) -> None:
         """The dense-slice sink protocol: slices [k, *slice_shape] (left unchanged)."""
@@ -226,16 +234,19 @@ class SparseSliceStream:
             self._deliver((self.next + j) % len(self.slots))
         st = int(self.status.item())
         if st:
+            self.status.zero_()  # reported once: later drains of good windows succeed
             raise RuntimeError(f"glide_footprint_compact reported status {st:#x}")
 
 
 class ReleaseAssembler:
     """An ``on_host`` consumer of ``SparseSliceStream``: keeps each release's sparse slices
     until all ``n_time_bins`` of them have arrived, then calls ``write_release(r, block)``
-    with the dense ``[T, *slice_shape]`` float32 block. ``finish()`` writes the releases
-    still open (bins that never arrived are zero)."""
+    with the dense ``[T, *slice_shape]`` block (float32, or ``dtype``). ``finish()`` writes
+    the releases still open (bins that never arrived are zero)."""
 
-    def __init__(self, n_time_bins: int, slice_shape: tuple, write_release: Callable[[int, np.ndarray], None]) -> None:
+    def __init__(self, n_time_bins: int, slice_shape: tuple, write_release: Callable[[int, np.ndarray], None],
+                 dtype=np.float32) -> None:
+        self.dtype = np.dtype(dtype)
         self.n_time_bins = int(n_time_bins)
         self.slice_shape = tuple(int(s) for s in slice_shape)
         self.write_release = write_release
@@ -248,13 +259,13 @@ class ReleaseAssembler:
             bins = self.open.setdefault(int(r), {})
             # copies: the arrays handed in are only valid during the call
             bins.setdefault(int(b), []).append((np.array(cell[a:e], dtype=np.int64),
-                                                np.array(value[a:e], dtype=np.float32)))
+                                                np.array(value[a:e], dtype=self.dtype)))
             if len(bins) == self.n_time_bins:
                 self._write(int(r))
 
     def _write(self, r: int) -> None:
         bins = self.open.pop(r)
-        block = np.zeros((self.n_time_bins, int(np.prod(self.slice_shape))), dtype=np.float32)
+        block = np.zeros((self.n_time_bins, int(np.prod(self.slice_shape))), dtype=self.dtype)
         for b, parts in bins.items():
             (c, v), rest = parts[0], parts[1:]
             block[b, c] = v  # assigned, not added: the values land bit-unchanged

@@ -159,6 +159,9 @@ class PackedWindow:
         self.wind = torch.empty(wb.value, dtype=torch.uint8, device=device)
         self.surf = torch.empty(sb.value, dtype=torch.uint8, device=device)
         self.support = torch.empty(pb.value, dtype=torch.uint8, device=device)
+        # sums of u, v, w of the start and end snapshots over all cells (the grid means of the
+        # runtime's wind diagnostic), written by pack()
+        self.wind_sum = torch.zeros(6, dtype=torch.float64, device=device)
         self.key = None
 
     @property
@@ -189,6 +192,9 @@ class PackedWindow:
         d.wind_packed = self.wind.data_ptr()
         d.surf_packed = self.surf.data_ptr()
         d.support_packed = self.support.data_ptr()
+        d.wind_sum = self.wind_sum.data_ptr()
+        with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+            self.wind_sum.zero_()
         _abi.check(_abi.lib.glide_window_pack(C.byref(d), stream_handle(stream)), "glide_window_pack")
         self.key = wf.time_start
 

@@ -87,6 +87,11 @@ typedef struct glide_window_desc {
     void* wind_packed;           /* [nz][ny][nx][8]: u0 v0 w0 u1 v1 w1 - - */
     void* surf_packed;           /* [ny][nx][16]: blh sp ustar shf t - - - (start), same (end) */
     void* support_packed;        /* [nz][ny][nx][8]: ft_sigma_w ft_T_Lw rho drho/dz meander_su meander_sv - - */
+    /* optional output, device [6] float64 (added to; NULL = not computed): the sums over all
+     * nz * ny * nx cells of u, v, w of the start snapshot, then of the end snapshot. Divided by
+     * the cell count they are the grid means behind the runtime's per-step wind diagnostic
+     * (_advection_alpha_wind_mean, src/lpdm/main.py:892-938). */
+    double* wind_sum;
 } glide_window_desc;
 
 /* Per-outer-step schedule entry, computed on the host exactly as the
@@ -107,6 +112,10 @@ typedef struct glide_footprint_grid {
      * time-ago slices per release, [n_releases][k][n_z][n_y][n_x], bin t stored in
      * slot t % k; the caller flushes a slot once its bin can no longer be reached. */
     int32_t ring;
+    /* 0: float32 footprint values; 1: float64 values, each contribution weight * dt
+     * formed and summed in FP64 (FootprintGridder(dtype=torch.float64),
+     * src/lpdm/footprint_gridder.py:50-115) */
+    int32_t value_f64;
 } glide_footprint_grid;
 
 typedef struct glide_step_args {
@@ -139,7 +148,8 @@ typedef struct glide_step_args {
      * Philox-4x32-10 draws keyed by seed and counted by (particle, step_index). */
     const float* noise_substep; const float* noise_meander; uint64_t seed;
     /* post-step (footprint + escape kill) */
-    float* footprint;                        /* [R][T][Zb][Y][X], may be NULL (no accumulation) */
+    void* footprint;                         /* [R][T][Zb][Y][X] float32 (float64 when fp.value_f64),
+                                              * may be NULL (no accumulation) */
     glide_footprint_grid fp;
     double dom_lon_min, dom_lon_max, dom_lat_min, dom_lat_max, dom_alt_max;
     int32_t* escaped_per_step;               /* [n_steps] counters (added to), may be NULL */
@@ -167,6 +177,12 @@ typedef struct glide_step_args {
     const void* conv_column; int32_t conv_step; int32_t conv_nz;
     const float* conv_uniforms;   /* injected uniforms [2][n], or NULL: Philox keyed by seed */
     int32_t* conv_moved;          /* device counter of moved particles (added to), may be NULL */
+    /* optional per-step diagnostic, device [n_steps][3] float64 (added to; NULL = none): the
+     * sums of lon, lat and z over all n particles (active or not) after each step's
+     * post-step; divided by n they are the runtime's mean-position diagnostic
+     * (particles[:, :3].mean(0), src/lpdm/main.py:1565-1566). Only steps j >= post_begin
+     * are summed; n_steps is then at most 1535. */
+    double* diag_pos_sum;
 } glide_step_args;
 
 /* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */
@@ -225,9 +241,9 @@ typedef struct glide_regrid_args {
 
 /* Sparse form of completed footprint slices (glide_footprint_compact). A slice is one
  * (release, time_ago) block [n_z][n_y][n_x] of the footprint, stored as one row of
- * `cells` float32. Device memory throughout. */
+ * `cells` float32 (float64 when value_f64). Device memory throughout. */
 typedef struct glide_compact_args {
-    float* rows;                   /* [n_rows][cells] slices; cleared entries are set to 0 */
+    void* rows;                    /* [n_rows][cells] slices; cleared entries are set to 0 */
     int64_t n_rows;
     int64_t cells;                 /* values per slice, 1 .. INT32_MAX */
     const int64_t* row_index;      /* [k] rows to compact, in output order */
@@ -235,10 +251,11 @@ typedef struct glide_compact_args {
     int32_t clear;                 /* != 0: set every compacted row to 0 (the rows must be distinct) */
     int64_t* slice_offset;         /* [k + 1] out: slice s holds entries [slice_offset[s], slice_offset[s+1]) */
     int32_t* out_cell;             /* [capacity] out: cell index within the slice, ascending per slice */
-    float* out_value;              /* [capacity] out: the value, bit-unchanged */
+    void* out_value;               /* [capacity] out: the value, bit-unchanged (float32 or float64) */
     int64_t capacity;
     uint32_t* status;              /* device status word (GLIDE_STATUS_*), may be NULL */
     void* scratch; size_t scratch_bytes;  /* glide_footprint_compact_scratch_bytes(k, cells) */
+    int32_t value_f64;             /* 1: rows and out_value hold float64 values (8-byte words) */
 } glide_compact_args;
 
 /* --- library ------------------------------------------------------------------ */
@@ -333,19 +350,20 @@ glide_status glide_agl_regrid(const glide_regrid_args* args, void* stream);
 /* --- footprint accumulation alone -----------------------------------------------
  * FootprintGridder.accumulate (src/lpdm/footprint_gridder.py:117-197) for the
  * per-step plug-in path. t_idx and release_idx are int32 [n]; positions follow
- * pos_stride as in glide_step_args. */
+ * pos_stride as in glide_step_args. The footprint holds float32 values, or float64
+ * when grid->value_f64 (weight * dt formed and added in FP64). */
 glide_status glide_footprint_accumulate(int64_t n, const float* lon, const float* lat, const float* z,
                                         int64_t pos_stride, const uint8_t* active, const float* weights,
                                         int64_t weight_stride, const int32_t* t_idx,
                                         const int32_t* release_idx, float dt_seconds,
-                                        const glide_footprint_grid* grid, float* footprint, void* stream);
+                                        const glide_footprint_grid* grid, void* footprint, void* stream);
 
 /* --- sparse footprint slices -----------------------------------------------------
  * The device half of streaming completed footprint slices to the output writer
  * (OutputWriter.write_footprint_region, src/lpdm/output_writer.py:215-243, which takes
  * dense (release, T, Z, Y, X) blocks): most cells of a slice are zero, so the slices
  * leave the device as (cell, value) lists. Entry e of the output is a cell whose float32
- * bit pattern is not zero (so -0.0 and NaN are kept and a dense slice is rebuilt
+ * (float64 when value_f64) bit pattern is not zero (so -0.0 and NaN are kept and a dense slice is rebuilt
  * bit-exactly by writing the values into zeros); slices in row_index order, cells
  * ascending within a slice. A row outside [0, n_rows) sets GLIDE_STATUS_BAD_ROW and
  * yields an empty slice. slice_offset is always written; when its last entry (the total)
@@ -383,8 +401,11 @@ glide_status glide_convect_redistribute(const glide_convect_args* args, void* st
  * lives in one static device array of the library, sized for at most
  * GLIDE_CONVECT_NOALLOC_MAX_NZ levels (135 KB, held by every GPU that loads the
  * library until exit); larger grids are rejected with GLIDE_ERR_INVALID_ARG.
- * The first call on each device looks up that array's device address with the
- * device current; make that first call before any stream capture. All calls
+ * Every call made outside stream capture looks up that array's device address
+ * on the current device (so a device reset, which reloads the library's module
+ * and may move the array, is followed by the next such call); a call on a
+ * capturing stream reuses the address the last uncaptured call on that device
+ * found, so make the first call on each device before any stream capture. All calls
  * share the array: two calls that may run at the same time on the GPU (streams
  * not ordered with each other) race on it. Each call writes every part of the
  * array it reads before reading it, so nothing needs clearing between calls.

@@ -21,7 +21,7 @@ def grid_of(run: GoldenRun) -> GridInfo:
 def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool = True, met_dtype: str = "f32",
                seed: int = 1234, hanna_kw: dict | None = None, launch_variant: int = 0,
                reorder: bool = True, steps_per_launch: int | None = None,
-               fuse_convection: bool = True) -> BatchRunner:
+               fuse_convection: bool = True, fp_dtype: str = "f32") -> BatchRunner:
     z = run.z
     m = run.met
     grid = grid_of(run).to_device(device)
@@ -54,7 +54,7 @@ def runner_for(run: GoldenRun, device, *, step_offset: int = 0, injected: bool =
         grid=grid, window_provider=window_provider,
         hanna=HannaConfig(meander_enabled=bool(z["meander"]), max_substeps=ms, **(hanna_kw or {})),
         footprint=FootprintSpec(tuple(z["grid_lon"]), tuple(z["grid_lat"]), int(nxy[0]), int(nxy[1]),
-                                tuple(float(e) for e in z["grid_z"]), int(nxy[2]), n_rel),
+                                tuple(float(e) for e in z["grid_z"]), int(nxy[2]), n_rel, value_dtype=fp_dtype),
         domain=DomainSpec(tuple(z["dom_lon"]), tuple(z["dom_lat"]), float(z["dom_alt"])),
         emanuel=EmanuelConfig() if bool(z["convection"]) else None,
         met_dtype=met_dtype, device=device, seed=seed,
