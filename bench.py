@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
     ap.add_argument("--workload", default="single-site",
-                    choices=["single-site", "multisite", "serving", "precision", "regrid"],
+                    choices=["single-site", "multisite", "serving", "precision", "regrid", "periodic"],
                     help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints; "
                          "serving: Poisson stream of footprint requests through FootprintServer")
     ap.add_argument("--requests", type=int, default=2000)
@@ -84,6 +84,10 @@ def parse():
     ap.add_argument("--sites", type=int, default=56)
     ap.add_argument("--release-times", type=int, default=48)
     ap.add_argument("--days", type=float, default=5.0)
+    ap.add_argument("--periodic-releases", type=int, default=720,
+                    help="periodic: hourly releases of 20,000 particles (the reference's example has 720)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the extra jobs (reference GPU path, multisite, periodic)")
     ap.add_argument("--dense-footprints", action="store_true",
                     help="multisite: move completed slices to the host dense (default: as (cell, value) lists)")
     return ap.parse_args()
@@ -92,7 +96,7 @@ def parse():
 def workload(n_particles: int, rank: int = 0, n_snapshots: int = 26):
     import dataclasses
 
-    from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.config import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
     from glide_b200.synthetic import config_met_spec
 
     spec = config_met_spec(1, n_snapshots=26)
@@ -120,20 +124,24 @@ def workload(n_particles: int, rank: int = 0, n_snapshots: int = 26):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    """nvidia-smi clock / throttle-reason sampling during the timed region (samples go to a
+    CSV in the system temp directory, or in GLIDE_BENCH_CLOCKS_DIR when set)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int) -> None:
+        import tempfile
+
         self.gpu = gpu_index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+        out = os.environ.get("GLIDE_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = Path(out) / f"glide_bench_clocks_gpu{gpu_index}_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.gpu), "-lms", "20"], stdout=self.f,
@@ -311,7 +319,7 @@ def multisite_workload(args, rank: int = 0):
     time_ago footprint per release kept as two live slices (ring)."""
     import dataclasses
 
-    from glide_b200.runtime import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.config import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
     from glide_b200.synthetic import config_met_spec
 
     rng = np.random.default_rng(20261206 + rank)
@@ -350,7 +358,7 @@ def multisite_workload(args, rank: int = 0):
     return cfg
 
 
-def run_multisite(args) -> None:
+def run_multisite(args, emit: bool = True) -> dict:
     """The batched multi-release job: every release in one particle batch, one fused
     launch per met window, completed time_ago slices streamed to pinned host memory
     (compacted to (cell, value) lists on the device unless --dense-footprints)."""
@@ -430,7 +438,145 @@ def run_multisite(args) -> None:
     if not args.dense_footprints:
         line.update({"footprint_dense_bytes": to_host.dense_bytes, "footprint_entries": to_host.entries,
                      "footprint_total_host": host_total[0], "short_copies": to_host.short_copies})
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+PERIODIC_SITE = (-9.9046, 53.3267)  # Mace Head, the reference's periodic example
+PERIODIC_MET_PERIOD_H = 168
+
+
+def periodic_workload(args, rank: int = 0):
+    """The reference's periodic single-site job (configs/example_mhd_january_periodic.yaml):
+    720 hourly 1 h releases of 20,000 particles at 10 m AGL at one site, each integrated
+    5 days backward at dt = 60 s with meander and Emanuel convection, a time-integrated
+    footprint (n_time_bins 1) in three layers (0-40 m, 40 m-1 km, 1-5 km) on the
+    EUROPE-box grid. The synthetic met (60 x 281 x 401) has 169 hourly snapshots; the
+    job's 840 hours use them cyclically (hour h reads window h mod 168)."""
+    import dataclasses
+
+    from glide_b200.config import DomainSpec, EmanuelConfig, FootprintSpec, HannaConfig
+    from glide_b200.synthetic import config_met_spec
+
+    rng = np.random.default_rng(20261207 + rank)
+    n_rel, per = args.periodic_releases, 20_000
+    length_s = 5 * 86400.0
+    base = config_met_spec(1)
+    spec = dataclasses.replace(base, n_snapshots=PERIODIC_MET_PERIOD_H + 1, seed=20261207 + rank)
+    t_rel0 = base.start_time + timedelta(hours=121)
+    n = n_rel * per
+    parts = np.empty((n, 4), dtype=np.float32)
+    parts[:, 0], parts[:, 1], parts[:, 2], parts[:, 3] = PERIODIC_SITE[0], PERIODIC_SITE[1], 10.0, 1.0 / per
+    k = np.repeat(np.arange(n_rel - 1, -1, -1), per)  # latest releases first: they activate first walking backward
+    rel_off = (k * 3600.0 + rng.uniform(0.0, 3600.0, n)).astype(np.float32)
+    cfg = dict(
+        spec=spec, particles=parts, rel_off=rel_off, win_end=(k * 3600.0 + 3600.0).astype(np.float32),
+        ridx=k.astype(np.int32), n_releases=n_rel, per_release=per,
+        batch_start=t_rel0, cursor_start=t_rel0 + timedelta(hours=n_rel),
+        terminus=t_rel0 + timedelta(hours=1) - timedelta(seconds=length_s), length_s=length_s, dt_s=60.0,
+        hanna=HannaConfig(meander_enabled=True, max_substeps=6), emanuel=EmanuelConfig(),
+        footprint=FootprintSpec((-60.125, 40.125), (9.875, 80.125), 401, 281, (0.0, 40.0, 1000.0, 5000.0), 1, n_rel),
+        domain=DomainSpec((-60.0, 40.0), (10.0, 80.0), 15000.0),
+    )
+    return cfg
+
+
+def _cyclic_index(syn):
+    def index_of(hour):
+        return syn.window_index(hour) % PERIODIC_MET_PERIOD_H
+
+    return index_of
+
+
+def _cyclic_provider(syn, grid):
+    """Window provider of the periodic job: window h of the synthetic met (h = the hour's
+    index mod the period) stamped with the requested hour."""
+    from glide_b200.window import Snapshot, WindowFields
+
+    lowest = int(np.argmin(syn.levels))
+    index_of = _cyclic_index(syn)
+
+    def provider(hour):
+        h = index_of(hour)
+        snaps = []
+        for kk, t in ((h, hour), (h + 1, hour + timedelta(hours=1))):
+            f = dict(syn.fields[kk])
+            f["t_lowest"] = f["t"][lowest]
+            snaps.append(Snapshot(t, f))
+        return WindowFields(snaps[0], snaps[1], grid, None)
+
+    return provider
+
+
+def run_periodic(args, emit: bool = True, with_reference: bool = True) -> dict:
+    """The 720-release, 5-day job in one batch (one fused launch per met window, bf16
+    met by default), timed whole with CUDA events: footprints/s and active
+    particle-steps/s. Beside it, the reference's CUDA-graph path on one of the batches
+    its runtime would run (24 releases, one calendar day: 480,000 particles), timed on 240
+    steps once all of them are released."""
+    import torch
+
+    from glide_b200.runtime import BatchRunner, ParticleState
+    from glide_b200.synthetic import SyntheticMet
+    from glide_b200.window import grid_from_synthetic
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = periodic_workload(args)
+    t_gen = time.perf_counter()
+    syn = SyntheticMet(cfg["spec"], device=dev)
+    t_gen = time.perf_counter() - t_gen
+    grid = grid_from_synthetic(syn).to_device(dev)
+    met = args.met if args.met != "f32" else "bf16"
+    runner = BatchRunner(grid=grid, window_provider=_cyclic_provider(syn, grid), hanna=cfg["hanna"],
+                         footprint=cfg["footprint"], domain=cfg["domain"], emanuel=cfg["emanuel"], met_dtype=met,
+                         device=dev, seed=91)
+    state = ParticleState.from_particles(cfg["particles"], cfg["rel_off"], cfg["win_end"], cfg["ridx"], dev)
+    run = runner.start(state, batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"],
+                       cursor_terminus=cfg["terminus"], sim_length_s=cfg["length_s"], dt_seconds=cfg["dt_s"])
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t_wall = time.perf_counter()
+    with ClockSampler(0) as clocks:
+        e0.record(stream)
+        out = run.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    t = e0.elapsed_time(e1) / 1e3
+    act = out.active_per_step.astype(np.int64)
+    active_ps = int(act.sum())
+    fp_total = float(out.footprint.sum(dtype=torch.float64).item())
+    line = {"workload": "periodic", "metric": "footprints/s", "value": cfg["n_releases"] / t, "unit": "footprints/s",
+            "active_particle_steps_per_s": active_ps / t, "releases": cfg["n_releases"],
+            "particles": int(cfg["particles"].shape[0]), "outer_steps": out.n_steps, "windows": len(run.windows),
+            "active_particle_steps": active_ps, "device_s": t, "wall_s": wall, "met_generation_s": t_gen,
+            "met": met, "dt_s": cfg["dt_s"], "status": out.status, "escaped": int(out.escaped_per_step.sum()),
+            "footprint_total": fp_total, "clocks": clocks.summary(),
+            "config": "720 hourly releases x 20,000 particles at (-9.9046, 53.3267) 10 m, 5 days backward, dt 60 s, "
+                      "meander + convection, time-integrated 3-layer footprint, 60x281x401 synthetic met "
+                      f"({PERIODIC_MET_PERIOD_H + 1} snapshots used cyclically)"}
+    del out, run, state, runner
+    torch.cuda.empty_cache()
+    if with_reference and _reference_modules() is not None:
+        day = 24
+        sel = cfg["ridx"] < day  # the first calendar day's releases: one batch of the reference's runtime
+        rcfg = dict(cfg, particles=cfg["particles"][sel], rel_off=cfg["rel_off"][sel], win_end=cfg["win_end"][sel],
+                    ridx=cfg["ridx"][sel])
+        res = reference_cuda_graph_rate(rcfg, _reference_window_fn(syn, _cyclic_index(syn)),
+                                        cursor_start=cfg["batch_start"], n_warm=130, n_time=240, dt_s=cfg["dt_s"],
+                                        sim_length_s=cfg["length_s"])
+        res["slice"] = ("one day's batch (24 releases x 20,000 particles, all released), 240 steps from the "
+                        "batch's first release hour backward after 130 untimed; f32 met (the reference's)")
+        line["reference_gpu"] = res
+        if "value" in res:
+            line["vs_reference_gpu"] = line["active_particle_steps_per_s"] / res["value"]
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_regrid(args) -> None:
@@ -568,29 +714,27 @@ def run_serving(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args) -> None:
-    """The reference's own GPU path on this workload: its HannaScheme static step core
-    compiled with torch.compile(mode="reduce-overhead") (GLIDE_COMPILE=1), its Emanuel
-    convection, FootprintGridder and escape kill, driven step by step as its cursor
-    loop does (main.py:1382-1477), with its own RNG. Needs the reference installed in
-    baseline/_ref (pip install --no-deps --target baseline/_ref <reference>). The hot
-    path imports xarray only for annotations; a two-class stand-in module is supplied."""
-    import tempfile
+_REF_MODULES = None
 
-    os.environ["GLIDE_COMPILE"] = "1"
+
+def _reference_modules():
+    """The reference's modules from the pip-installed copy in baseline/_ref (its hot path
+    imports xarray only for annotations; a two-class stand-in module is supplied), or
+    None when it is not installed."""
+    global _REF_MODULES
+    if _REF_MODULES is not None:
+        return _REF_MODULES
+    import tempfile
+    from types import SimpleNamespace
+
     ref = ROOT / "baseline" / "_ref"
     if not (ref / "lpdm").is_dir():
-        print(json.dumps({"impl": "reference-gpu", "unavailable": "reference not installed in baseline/_ref"}))
-        return
+        return None
     stub = Path(tempfile.mkdtemp(prefix="glide_xr_"))
     (stub / "xarray").mkdir()
     (stub / "xarray" / "__init__.py").write_text("class Dataset:\n    pass\n\n\nclass DataArray:\n    pass\n")
     sys.path.insert(0, str(ref))
     sys.path.insert(0, str(stub))
-    from types import SimpleNamespace
-
-    import torch
-
     import lpdm.convection.emanuel as em
     import lpdm.footprint_gridder as fg
     import lpdm.gpu_engine as ge
@@ -598,78 +742,142 @@ def run_reference_gpu(args) -> None:
     import lpdm.met_reader as mr
     import lpdm.turbulence.hanna as hn
 
-    from glide_b200.synthetic import SyntheticMet
+    _REF_MODULES = SimpleNamespace(em=em, fg=fg, ge=ge, lm=lm, mr=mr, hn=hn)
+    return _REF_MODULES
 
-    n = args.particles
-    cfg = workload(n, 0, n_snapshots=max(5, args.snapshots if args.snapshots < 26 else 5))
+
+def reference_cuda_graph_rate(cfg, window_fn, *, cursor_start, n_warm: int, n_time: int, dt_s: float,
+                              sim_length_s: float) -> dict:
+    """The reference's own GPU path on a workload: its HannaScheme static step core compiled
+    with torch.compile(mode="reduce-overhead") (the CUDA-graph path of GLIDE_COMPILE=1),
+    its Emanuel convection once per window, FootprintGridder and the escape kill, driven
+    step by step as its cursor loop does (main.py:1382-1477) with its own RNG, on all of
+    ``cfg``'s particles from ``cursor_start``. ``window_fn(hour)`` gives the reference's
+    ``HourlyMetTensors`` (host tensors) of the window starting at ``hour``. Times ``n_time``
+    steps after ``n_warm`` (the compile, the first window) with CUDA events; the value is
+    active particle-steps per second."""
+    import torch
+
+    ref = _reference_modules()
+    if ref is None:
+        return {"unavailable": "reference not installed in baseline/_ref"}
     dev = torch.device("cuda")
-    syn = SyntheticMet(cfg["spec"], device=dev)
-
-    def ref_window(h):
-        w = syn.window(h, device="cpu")
-        md = w.metadata
-        return mr.HourlyMetTensors(
-            hour_start=w.hour_start.contiguous(), hour_end=w.hour_end.contiguous(),
-            metadata=mr.MetFieldMetadata(lon=md.lon, lat=md.lat, level=md.level,
-                                         pressure_level_hpa=md.pressure_level_hpa, time_start=md.time_start,
-                                         time_end=md.time_end, variable_units=dict(md.variable_units)),
-            channel_names=w.channel_names, height_agl_m=w.height_agl_m.contiguous())
-
-    scheme = hn.HannaScheme(meander_enabled=True, max_substeps=6)
-    conv = em.EmanuelReducedConvection()
-    engine = ge.GPUEngine(device="cuda")
+    n = int(cfg["particles"].shape[0])
+    hc = cfg["hanna"]
+    scheme = ref.hn.HannaScheme(meander_enabled=hc.meander_enabled, max_substeps=hc.max_substeps)
+    conv = ref.em.EmanuelReducedConvection() if cfg.get("emanuel") is not None else None
+    engine = ref.ge.GPUEngine(device="cuda", compile_hot_paths=True)
     fp = cfg["footprint"]
-    gridder = fg.FootprintGridder(lon_bounds=fp.lon_bounds, lat_bounds=fp.lat_bounds, z_edges_m=fp.z_edges,
-                                  n_time_bins=fp.n_time_bins, n_y=fp.n_y, n_x=fp.n_x, n_releases=1, device=dev)
+    gridder = ref.fg.FootprintGridder(lon_bounds=fp.lon_bounds, lat_bounds=fp.lat_bounds, z_edges_m=fp.z_edges,
+                                      n_time_bins=fp.n_time_bins, n_y=fp.n_y, n_x=fp.n_x,
+                                      n_releases=int(cfg["ridx"].max()) + 1, device=dev)
     dom = cfg["domain"]
+    from types import SimpleNamespace
+
     mcfg = SimpleNamespace(met_domain=SimpleNamespace(lon_bounds=dom.lon_bounds, lat_bounds=dom.lat_bounds,
                                                       alt_max_m=dom.alt_max_m))
     p = torch.as_tensor(cfg["particles"], device=dev)
     rel = torch.as_tensor(cfg["rel_off"], device=dev)
     wend = torch.as_tensor(cfg["win_end"], device=dev)
-    ridx = torch.zeros(n, dtype=torch.int64, device=dev)
+    ridx = torch.as_tensor(cfg["ridx"], device=dev).to(torch.int64)
     state = scheme.initialize_state(n, device=dev, dtype=torch.float32)
     alive = torch.ones(n, dtype=torch.bool, device=dev)
-    t_cursor, term = cfg["cursor_start"], cfg["terminus"]
+    t_cursor, term = cursor_start, cfg["terminus"]
     bstart = cfg["batch_start"].timestamp()
     windows: dict = {}
     last = None
     wcache: dict = {}
-    n_warm = 130  # the compile, the one-step first window and a full window
-    n_time = 240
+    active_steps = torch.zeros((), dtype=torch.int64, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t_wall = time.perf_counter()
     for k in range(n_warm + n_time):
         if k == n_warm:
             torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
+            active_steps.zero_()
             e0.record()
-        delta = min(DT_S, (t_cursor - term).total_seconds())
+        delta = min(dt_s, (t_cursor - term).total_seconds())
         cur = t_cursor.timestamp() - bstart
-        active = (rel >= cur) & (rel - SIM_LENGTH_S <= cur) & alive
-        h = syn.window_index(lm._hour_floor(t_cursor))
-        if h not in windows:
+        active = (rel >= cur) & (rel - sim_length_s <= cur) & alive
+        hour = ref.lm._hour_floor(t_cursor)
+        if hour not in windows:
             windows.clear()
-            windows[h] = ref_window(h)
-        win = windows[h]
-        alpha, _ = lm._advection_alpha_wind_mean(win, t_cursor, delta, dev, torch.float32, wcache)
+            windows[hour] = window_fn(hour)
+        win = windows[hour]
+        alpha, _ = ref.lm._advection_alpha_wind_mean(win, t_cursor, delta, dev, torch.float32, wcache)
         p, state = scheme.step(particles=p, state=state, met_window=win, t_alpha=alpha, dt_seconds=delta,
                                active_mask=active, engine=engine)
         if win.metadata.time_start != last:
-            p, _ = conv.maybe_convect(particles=p, state={}, met_window=win, t_alpha=alpha, dt_seconds=delta,
-                                      active_mask=active, engine=engine)
+            if conv is not None:
+                p, _ = conv.maybe_convect(particles=p, state={}, met_window=win, t_alpha=alpha, dt_seconds=delta,
+                                          active_mask=active, engine=engine)
             last = win.metadata.time_start
         t_idx = ((wend - cur).clamp_(min=0.0) / 3600.0).floor().to(torch.int64)
+        if gridder.n_t == 1:
+            t_idx.clamp_(max=0)
         gridder.accumulate(particles=p[:, :3], active_mask=active, weights=p[:, 3], t_idx=t_idx, release_idx=ridx,
                            dt_seconds=delta)
-        alive = alive & ~(active & ~lm._within_met_domain(p, mcfg))
+        alive = alive & ~(active & ~ref.lm._within_met_domain(p, mcfg))
+        active_steps += active.sum()
         t_cursor = t_cursor - timedelta(seconds=delta)
-    e1 = torch.cuda.Event(enable_timing=True)
     e1.record()
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3
-    value = n * n_time / t
+    act = int(active_steps.item())
+    return {"value": act / t, "unit": "active particle-steps/s", "particles": n, "steps": n_time,
+            "warmup": n_warm, "ms_per_step": 1e3 * t / n_time, "active_particle_steps": act,
+            "graph_state": scheme._graph_compile_state, "wall_s": time.perf_counter() - t_wall}
+
+
+def _reference_window_fn(syn, index_of=None):
+    """``window_fn`` of reference_cuda_graph_rate from a SyntheticMet: the window starting
+    at an hour as the reference's ``HourlyMetTensors`` on the host; ``index_of(hour)`` maps
+    the hour to the synthetic window index (default: ``syn.window_index``)."""
+    def window_fn(hour):
+        ref = _reference_modules()
+        h = syn.window_index(hour) if index_of is None else index_of(hour)
+        w = syn.window(h, device="cpu")
+        md = w.metadata
+        return ref.mr.HourlyMetTensors(
+            hour_start=w.hour_start.contiguous(), hour_end=w.hour_end.contiguous(),
+            metadata=ref.mr.MetFieldMetadata(lon=md.lon, lat=md.lat, level=md.level,
+                                             pressure_level_hpa=md.pressure_level_hpa, time_start=hour,
+                                             time_end=hour + timedelta(hours=1),
+                                             variable_units=dict(md.variable_units)),
+            channel_names=w.channel_names, height_agl_m=w.height_agl_m.contiguous())
+
+    return window_fn
+
+
+def single_site_reference_gpu(syn, cfg, n_warm: int = 130, n_time: int = 240) -> dict:
+    """The reference's CUDA-graph path on the single-site workload, from the release end:
+    the first 130 steps (the compile, the one-step first window and a full window) untimed,
+    the next 240 timed, when every particle of the 1 h release is active."""
+    res = reference_cuda_graph_rate(cfg, _reference_window_fn(syn), cursor_start=cfg["cursor_start"],
+                                    n_warm=n_warm, n_time=n_time, dt_s=DT_S, sim_length_s=SIM_LENGTH_S)
+    if "value" in res:
+        res["particle_steps_per_s"] = int(cfg["particles"].shape[0]) * n_time / (res["ms_per_step"] * n_time / 1e3)
+    return res
+
+
+def run_reference_gpu(args) -> None:
+    """``--impl reference-gpu``: the reference's own torch.compile CUDA-graph step path
+    (installed in baseline/_ref) on the single-site workload."""
+    import torch
+
+    from glide_b200.synthetic import SyntheticMet
+
+    n = args.particles
+    cfg = workload(n, 0, n_snapshots=max(5, args.snapshots if args.snapshots < 26 else 5))
+    syn = SyntheticMet(cfg["spec"], device=torch.device("cuda"))
+    res = single_site_reference_gpu(syn, cfg)
+    if "unavailable" in res:
+        print(json.dumps({"impl": "reference-gpu", **res}))
+        return
+    value = res["particle_steps_per_s"]
     print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
-                      "steps": n_time, "warmup": n_warm, "ms_per_step": 1e3 * t / n_time, "higher_is_better": True,
-                      "dtype": "f32", "data": "synthetic", "graph_state": scheme._graph_compile_state,
+                      "steps": res["steps"], "warmup": res["warmup"], "ms_per_step": res["ms_per_step"],
+                      "higher_is_better": True, "dtype": "f32", "data": "synthetic", "graph_state": res["graph_state"],
                       "config": {"workload": "single-site 24 h backward, 200k particles, 60x281x401 met, dt 30 s",
                                  "step": "one outer step (the reference's graph replay + convection + gridder)"}}),
           flush=True)
@@ -792,6 +1000,9 @@ def main() -> None:
         return
     if args.workload == "multisite":
         run_multisite(args)
+        return
+    if args.workload == "periodic":
+        run_periodic(args)
         return
     if args.workload == "serving":
         run_serving(args)
@@ -968,10 +1179,44 @@ def main() -> None:
                                     "sample": f"{CPU_BASELINE_REPEATS} x {args.particles} particles x "
                                               f"{CPU_BASELINE_STEPS} outer steps, all "
                                               f"released (oracle port, {workers} processes, {wall:.1f} s)"}
+        if world == 1 and not args.no_extras:
+            line.update(run_extras(args, syn, cfg, value, line))
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_extras(args, syn, cfg, value: float, line: dict) -> dict:
+    """Extra jobs of the default run, beside the headline (each one's failure is recorded,
+    not raised): the reference's own CUDA-graph path on the same single-site workload and
+    B200, the 2,688-release multisite job and the 720-release periodic job (bf16 met)."""
+    import argparse
+
+    import torch
+
+    extras: dict = {}
+    t = time.perf_counter()
+    try:
+        ref = single_site_reference_gpu(syn, cfg)
+        if "particle_steps_per_s" in ref:
+            ref["vs_reference_gpu"] = value / ref["particle_steps_per_s"]
+            if "e2e" in line:
+                ref["e2e_vs_reference_gpu"] = line["e2e"]["value"] / ref["particle_steps_per_s"]
+        extras["reference_gpu"] = ref
+    except Exception as exc:  # noqa: BLE001 - an extra never costs the headline line
+        extras["reference_gpu"] = {"error": f"{type(exc).__name__}: {exc}"}
+    extras["reference_gpu"]["extra_wall_s"] = time.perf_counter() - t
+    torch.cuda.empty_cache()
+    for name, fn in (("multisite", run_multisite), ("periodic", run_periodic)):
+        t = time.perf_counter()
+        try:
+            extras[name] = fn(argparse.Namespace(**{**vars(args), "met": "bf16"}), emit=False)
+        except Exception as exc:  # noqa: BLE001
+            extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        extras[name]["extra_wall_s"] = time.perf_counter() - t
+        torch.cuda.empty_cache()
+    return extras
 
 
 def run_graph(cfg, syn, grid, make_runner, fresh_state, kw, dev, stream) -> dict:
