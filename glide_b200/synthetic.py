@@ -52,7 +52,13 @@ TWO_D = ("blh", "sp", "ustar", "shf")
 
 def stretched_agl_levels(n_levels: int, alt_max_m: float, first_layer_m: float = 10.0) -> np.ndarray:
     """Ascending AGL heights ``[n_levels]`` from 0 to ``alt_max_m``; the first layer is
-    ``first_layer_m`` thick and each higher layer a constant ratio thicker."""
+    ``first_layer_m`` thick and each higher layer a constant ratio thicker.
+
+    The benchmark levels are defined as the reference's ``stretched_agl_levels``
+    (src/lpdm/vertical_grid.py:70-144), so this follows its steps: the geometric-series
+    span in closed form, the ratio bracketed by doubling from [1, 2] and bisected 200
+    times, the cumulative sum of the layer thicknesses with the top pinned to
+    ``alt_max_m``."""
     if n_levels < 2:
         raise ValueError("n_levels must be >= 2")
     n_layers = n_levels - 1

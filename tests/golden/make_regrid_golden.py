@@ -49,7 +49,7 @@ def _case(rng, zp: int, ny: int, nx: int, toa_first: bool, lat_descending: bool)
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference source tree (holds src/lpdm)")
     args = ap.parse_args()
     sys.path.insert(0, str(Path(args.reference) / "src"))
     import torch
