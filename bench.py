@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--snapshots", type=int, default=26,
                     help="generate only the last N hourly snapshots (small profiling cases)")
     ap.add_argument("--workload", default="single-site",
-                    choices=["single-site", "multisite", "serving", "precision", "regrid", "periodic"],
+                    choices=["single-site", "multisite", "serving", "regrid", "periodic"],
                     help="multisite: 56 sites x 48 hourly releases, 5 days backward, ring footprints; "
                          "serving: Poisson stream of footprint requests through FootprintServer")
     ap.add_argument("--requests", type=int, default=2000)
@@ -883,115 +883,8 @@ def run_reference_gpu(args) -> None:
           flush=True)
 
 
-def run_precision(args) -> None:
-    """Precision sweep on the single-site workload: met stored float32, bf16 and fp16
-    (interpolation and integration in float32, convective column in FP64) against
-    the FP64 oracle on the same met, the same injected noise and uniforms, for a
-    subsample of the release (``--particles``, default 2,000) over 24 h. Reports
-    trajectory drift at 1, 6 and 24 h, footprint relative L1 and peak-cell error, and
-    drop counts."""
-    import torch
-
-    from glide_b200.runtime import BatchRunner, ParticleState
-    from glide_b200.synthetic import SyntheticMet
-    from glide_b200.window import grid_from_synthetic, window_from_synthetic
-    from oracle.convection import EmanuelParams
-    from oracle.hanna import HannaParams, StepNoise
-    from oracle.runtime import DomainSpec, GridSpec, run_batch
-
-    n = args.particles if args.particles != N_PARTICLES else 2000
-    dev = torch.device("cuda", 0)
-    cfg = workload(n)
-    syn = SyntheticMet(cfg["spec"], device=dev)
-    grid = grid_from_synthetic(syn).to_device(dev)
-    ms = 6
-    seed, cseed = 424242, 515151
-
-    def step_noise(k):
-        rng = np.random.default_rng([seed, k])
-        return rng.standard_normal((ms, 3, n), dtype=np.float32), rng.standard_normal((2, n), dtype=np.float32)
-
-    def uniforms(k):
-        rng = np.random.default_rng([cseed, k])
-        return rng.random(n, dtype=np.float32), rng.random(n, dtype=np.float32)
-
-    def noise_provider(steps):
-        sub, mea = zip(*(step_noise(k) for k in steps))
-        return torch.from_numpy(np.stack(sub)).to(dev), torch.from_numpy(np.stack(mea)).to(dev)
-
-    def conv_provider(k):
-        return torch.from_numpy(np.stack(uniforms(k))).to(dev)
-
-    marks = {"1h": 1 + 120, "6h": 1 + 6 * 120, "24h": 2880}
-    results = {}
-    for mode in ("f32", "bf16", "f16"):
-        r = BatchRunner(grid=grid, window_provider=lambda hk: window_from_synthetic(syn, syn.window_index(hk), grid),
-                        hanna=cfg["hanna"], footprint=cfg["footprint"], domain=cfg["domain"], emanuel=cfg["emanuel"],
-                        met_dtype=mode, device=dev, noise_provider=noise_provider, conv_uniform_provider=conv_provider)
-        st = ParticleState.from_particles(cfg["particles"], cfg["rel_off"], cfg["win_end"], cfg["ridx"], dev)
-        run = r.start(st, batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"],
-                      cursor_terminus=cfg["terminus"], sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S)
-        snaps = {}
-        while run.step_window():
-            done = run.windows[run.next_window - 1][1]
-            for name, k in marks.items():
-                if done == k:
-                    s = run.state
-                    snaps[name] = np.stack([s.lon.cpu().numpy(), s.lat.cpu().numpy(), s.z.cpu().numpy()])
-        out = run.finish()
-        results[mode] = dict(snaps=snaps, fp=out.footprint.cpu().numpy(), esc=int(out.escaped_per_step.sum()),
-                             status=out.status)
-    # FP64 oracle on the same met (copied from the device), noise and uniforms
-    cache = {}
-
-    def get_window(hk):
-        h = syn.window_index(hk)
-        if h not in cache:
-            cache.clear()
-            f0, f1 = syn.fields[h], syn.fields[h + 1]
-            w = {k: np.stack([f0[k].cpu().numpy(), f1[k].cpu().numpy()]) for k in f0}
-            w["height"] = syn.height_agl.cpu().numpy()
-            w.update(level=syn.levels, p_hpa=syn.pressure_level_hpa, lon=syn.lon, lat=syn.lat,
-                     time_start=syn.times[h], time_end=syn.times[h + 1])
-            cache[h] = w
-        return cache[h]
-
-    fp = cfg["footprint"]
-    dom = cfg["domain"]
-    t = time.perf_counter()
-    ora = run_batch(get_window=get_window, particles=cfg["particles"].T.copy(), rel_off=cfg["rel_off"],
-                    win_end_off=cfg["win_end"], release_idx=cfg["ridx"].astype(np.int64),
-                    batch_start=cfg["batch_start"], cursor_start=cfg["cursor_start"], cursor_terminus=cfg["terminus"],
-                    sim_length_s=SIM_LENGTH_S, dt_seconds=DT_S, params=HannaParams(meander_enabled=True, max_substeps=ms),
-                    grid=GridSpec(fp.lon_bounds, fp.lat_bounds, fp.n_x, fp.n_y, fp.z_edges, fp.n_time_bins, 1),
-                    domain=DomainSpec(dom.lon_bounds, dom.lat_bounds, dom.alt_max_m),
-                    noise_fn=lambda k: StepNoise(*step_noise(k)), emanuel=EmanuelParams(),
-                    conv_uniforms_fn=uniforms, dtype=np.float64, conv_dtype=np.float64,
-                    snapshot_steps=tuple(marks.values()))
-    t_oracle = time.perf_counter() - t
-    ofp = ora.footprint
-    line = {"workload": "precision", "particles": n, "oracle": "FP64 numpy oracle", "oracle_s": t_oracle,
-            "oracle_escaped": int(sum(ora.escaped_per_step)), "modes": {}}
-    for mode, res in results.items():
-        d = {"status": res["status"], "escaped": res["esc"]}
-        for name, k in marks.items():
-            a, b = res["snaps"][name], ora.snapshots[k][:3]
-            dx = (a[0] - b[0]) * 111320.0 * np.cos(np.deg2rad(b[1]))
-            dy = (a[1] - b[1]) * 110540.0
-            d[f"rms_horizontal_m_{name}"] = float(np.sqrt(np.mean(dx * dx + dy * dy)))
-            d[f"rms_vertical_m_{name}"] = float(np.sqrt(np.mean((a[2] - b[2]) ** 2)))
-            d[f"median_rel_{name}"] = float(np.median(np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1)))
-        d["footprint_rel_l1"] = float(np.abs(res["fp"] - ofp).sum() / np.abs(ofp).sum())
-        d["footprint_peak_rel_err"] = float(abs(res["fp"].max() - ofp.max()) / ofp.max())
-        line["modes"][mode] = d
-    print(json.dumps(line), flush=True)
-
-
 def main() -> None:
     args = parse()
-    if args.workload == "precision":
-        run_precision(args)
-        return
     if args.impl == "reference-gpu":
         run_reference_gpu(args)
         return
