@@ -22,7 +22,11 @@ synthetic met windows with ``glide_b200.synthetic``, and records:
   2 h backward from the release end (met regenerated from its seed).
 
 Every batch also records the runtime's per-step diagnostics (mean particle
-position, grid-mean wind; ``main.py:1565-1566``).
+position, grid-mean wind; ``main.py:1565-1566``) and the footprint of the same
+trajectories accumulated by the reference's gridder in float64
+(``out_footprint_f64``): the float32 gridder adds ~1e5 contributions per cell at the
+EUROPE-box case, and its round-off (1.7e-3 relative L1 there) is larger than the
+trajectories' differences.
 
 Noise is not stored: it is regenerated from the recorded seed by
 ``tests/golden/noise.py``.
@@ -342,6 +346,12 @@ def drive_batch(ref, case: str, noise_seed: int, device: str = "cpu", snap_every
     gridder = ref.fg.FootprintGridder(lon_bounds=grid["lon_bounds"], lat_bounds=grid["lat_bounds"],
                                       z_edges_m=grid["z_edges"], n_time_bins=grid["n_time_bins"],
                                       n_y=grid["n_y"], n_x=grid["n_x"], n_releases=len(rel), device=dev)
+    # the same gridder in float64 fed the same (float32) trajectories: the footprint without
+    # the float32 round-off of ~1e5 small additions per cell
+    gridder64 = ref.fg.FootprintGridder(lon_bounds=grid["lon_bounds"], lat_bounds=grid["lat_bounds"],
+                                        z_edges_m=grid["z_edges"], n_time_bins=grid["n_time_bins"],
+                                        n_y=grid["n_y"], n_x=grid["n_x"], n_releases=len(rel), device=dev,
+                                        dtype=torch.float64)
     cfg = SimpleNamespace(met_domain=SimpleNamespace(**domain))
     shim = _NoiseShim(ref, noise_seed, n, max_substeps)
     rshim = _RandShim(ref, noise_seed + 7) if convection else None
@@ -387,6 +397,8 @@ def drive_batch(ref, case: str, noise_seed: int, device: str = "cpu", snap_every
                 t_idx.clamp_(max=0)
             gridder.accumulate(particles=p[:, :3], active_mask=active, weights=p[:, 3], t_idx=t_idx,
                                release_idx=ridx_t, dt_seconds=delta)
+            gridder64.accumulate(particles=p[:, :3].double(), active_mask=active, weights=p[:, 3].double(),
+                                 t_idx=t_idx, release_idx=ridx_t, dt_seconds=delta)
             newly = active & ~ref.main._within_met_domain(p, cfg)
             alive = alive & ~newly
             esc.append(int(newly.sum()))
@@ -413,6 +425,7 @@ def drive_batch(ref, case: str, noise_seed: int, device: str = "cpu", snap_every
                dom_lon=np.array(domain["lon_bounds"]), dom_lat=np.array(domain["lat_bounds"]),
                dom_alt=np.array(domain["alt_max_m"]),
                out_particles=host(p).T.copy(), out_alive=host(alive), out_footprint=host(gridder.tensor),
+               out_footprint_f64=host(gridder64.tensor),
                out_escaped=np.array(esc), out_active=np.array(act), out_conv=np.array(conv_log).reshape(-1, 2),
                snap_steps=np.array([s for s, _ in snaps]), snap_particles=np.stack([a for _, a in snaps]),
                out_diag_pos=np.stack(diag_pos).astype(np.float32), out_diag_wind=np.stack(diag_wind).astype(np.float32),

@@ -348,7 +348,11 @@ def test_c1_batch_matches_reference_golden(cuda_device):
     """The benchmark's own configuration: 60 x 281 x 401 met, dt 30 s, meander and hourly
     convection on, 20,000 particles of the 100 m release, 2 h backward (every particle 1-2 h
     old at the end). Counts and the alive mask exact; trajectories within 1e-5 relative of
-    the reference's after 2 h for 99.5 % of the particles; footprint within 1e-4 relative L1;
+    the reference's after 2 h for 99.5 % of the particles (measured 99.8 %; the reference's
+    own CUDA path reaches 96.5 % against its CPU path); the footprint within 1e-4 relative
+    L1 of the reference's trajectories gridded in float64 (the kernel sums each particle's
+    residence in FP64), and within the float32 gridder's own round-off (1.7e-3 L1 from the
+    float64 gridding of the same trajectories) of the reference's float32 footprint;
     convection moved counts within rounding of the FP64 column CDF."""
     run = load_run("run_c1")
     out = run_gpu(run, cuda_device)
@@ -361,8 +365,10 @@ def test_c1_batch_matches_reference_golden(cuda_device):
     err = _scaled_err(parts, run["out_particles"])
     assert np.mean(err < 1e-5) >= 0.995, np.mean(err < 1e-5)
     assert np.median(err) < 1e-6, np.median(err)
+    r64 = run["out_footprint_f64"]
+    assert np.abs(fp - r64).sum() / np.abs(r64).sum() < 1e-4
     rfp = run["out_footprint"].astype(np.float64)
-    assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 1e-4
+    assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 3e-3
     moved = [int(m.item()) for _, m in out.convection]
     ref = [int(m) for _, m in run["out_conv"]]
     assert len(moved) == len(ref)

@@ -172,7 +172,8 @@ def test_c1_batch_matches_reference():
     """The single-site EUROPE-box case (60 x 281 x 401 met, dt 30 s, meander and hourly
     convection on; 20,000 particles, 2 h): counts and the alive mask exact, 99.5 % of the
     trajectories within 1e-5 relative of the reference after 2 h (measured 99.87 %), the
-    footprint within 1e-5 relative L1 (measured 7.7e-7), the diagnostics within 1e-6."""
+    footprint within 1e-5 relative L1 (measured 7.7e-7), in FP64 within 5e-5 of the
+    reference's float64 gridding, the diagnostics within 1e-6."""
     run = load_run("run_c1")
     res = run_batch(**oracle_kwargs(run))
     assert res.n_steps == int(run["n_steps"])
@@ -186,6 +187,12 @@ def test_c1_batch_matches_reference():
     assert np.mean(err < 1e-5) >= 0.995, np.mean(err < 1e-5)
     fp, rfp = res.footprint.astype(np.float64), run["out_footprint"].astype(np.float64)
     assert np.abs(fp - rfp).sum() / np.abs(rfp).sum() < 1e-5
+    # the FP64 gridder on the oracle's trajectories against the reference's float64 gridding
+    res64 = run_batch(**oracle_kwargs(run), fp_dtype=np.float64)
+    r64 = run["out_footprint_f64"]
+    # (measured 2.2e-5: the 0.1 % of trajectories that drift apart; the float32 footprints
+    # agree closer because the oracle adds in the reference's order and so repeats its round-off)
+    assert np.abs(res64.footprint - r64).sum() / np.abs(r64).sum() < 5e-5
     pos, wind = _diag_errors(res, run)
     assert pos.max() < 1e-6, pos.max()
     assert wind.max() < 5e-6, wind.max()
