@@ -302,9 +302,11 @@ __device__ __forceinline__ float noise_or_philox(const StepDev& p, const float* 
 // Launch shapes (threads per block, resident blocks per SM the register budget
 // is compiled for). Variant 0, 128 x 6 (<= 80 registers, 24 warps per SM), is
 // the measured default; the others exist for the autotuner: the best shape
-// depends on the particle count (wave quantisation of a batch across 148 SMs).
+// depends on the particle count (wave quantisation of a batch across 148 SMs) and
+// on the trade between resident warps and spills (128 x 7 and 896 x 1 cap the
+// kernel at 72 registers, 28 warps per SM, with a few spilled values).
 struct LaunchShape { int threads, min_blocks; };
-constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}, {768, 1}};
+constexpr LaunchShape kShapes[] = {{128, 6}, {64, 12}, {256, 3}, {128, 5}, {128, 8}, {768, 1}, {128, 7}, {896, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // variant kNumShapes: the general kernel at shape 0 whatever the arguments
 constexpr int kNumVariants = kNumShapes + 1;
@@ -734,6 +736,8 @@ static glide_status launch_step(const StepDev& d, cudaStream_t stream, int varia
         case 3: launch_shape<T, 3, false>(d, stream, smem); break;
         case 4: launch_shape<T, 4, false>(d, stream, smem); break;
         case 5: launch_shape<T, 5, false>(d, stream, smem); break;
+        case 6: launch_shape<T, 6, false>(d, stream, smem); break;
+        case 7: launch_shape<T, 7, false>(d, stream, smem); break;
         case kNumShapes: launch_shape<T, 0, true>(d, stream, smem); break;
         default: return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: launch_variant %d out of range", variant);
     }
