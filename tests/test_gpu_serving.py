@@ -91,3 +91,41 @@ def test_grouped_and_per_stream_servers_agree(met):
         a, b = g[k].footprint.numpy(), p[k].footprint.numpy()
         assert np.abs(a - b).sum() <= 1e-6 * max(np.abs(a).sum(), 1e-30)
 
+
+
+def test_budget_overfilled_with_more_than_a_grouped_launch(met, monkeypatch):
+    """60 requests against a budget that holds about 40 of them: admission stops at the
+    budget, more than 32 requests are in flight at once, so a tick's grouped launch is
+    split (glide_step_batched takes at most 32 batches), and every request's result is
+    still the one it has alone."""
+    from glide_b200 import serving
+    from glide_b200.serving import poisson_requests
+
+    syn, grid = met
+    sites = np.array([[0.0, 47.0], [5.0, 50.0], [-4.0, 45.0], [2.0, 43.0]])
+    reqs = poisson_requests(60, 1000.0, sites, syn.times[0] + timedelta(hours=4), 3.0, n_range=(300, 3000),
+                            duration_range_h=(2.0, 4.0), seed=23)
+    probe = _server(syn, grid, max_active=64)
+    sizes = sorted((probe.request_bytes(r) for r in reqs), reverse=True)
+    budget = float(sum(sizes[:40]))
+    groups: list[int] = []
+    real = serving.launch_grouped
+
+    def spy(args, stream):
+        groups.append(len(args))
+        return real(args, stream)
+
+    monkeypatch.setattr(serving, "launch_grouped", spy)
+    srv = _server(syn, grid, max_active=64, hbm_budget_bytes=budget)
+    res = {r.request_id: r for r in srv.serve(reqs, realtime=False)}
+    assert len(res) == len(reqs) and srv.stats.completed == len(reqs)
+    assert srv.stats.peak_bytes <= budget
+    assert srv.stats.peak_active > 32
+    assert max(groups) > 32  # a tick with more batches than one grouped launch holds
+    monkeypatch.setattr(serving, "launch_grouped", real)
+    for req in (reqs[0], reqs[33], reqs[59]):
+        alone = _server(syn, grid, max_active=1).serve([req], realtime=False)[0]
+        m = res[req.request_id]
+        assert alone.escaped == m.escaped and alone.active_particle_steps == m.active_particle_steps
+        a, b = alone.footprint.numpy(), m.footprint.numpy()
+        assert np.abs(a - b).sum() <= 1e-6 * max(np.abs(a).sum(), 1e-30)
