@@ -46,6 +46,13 @@ SITE = (-5.0, 52.0)
 # algorithmic bytes per particle-step (met gathers 200 values x b + 86 B of state, footprint, flags)
 B_ALG = {"f32": 200 * 4 + 86, "bf16": 200 * 2 + 86, "f16": 200 * 2 + 86}
 METRIC = "particle-steps/s"
+# From one ncu capture of the step kernel on this workload (float32 met, a window 7 h after
+# the release, 200,000 particles x 120 steps; profiles/step_kernel_single_site_f32.md):
+# DRAM bytes per launch and warp instructions issued per particle-step. The plume's met
+# is served from L1, so the kernel is bound by instruction issue, not by HBM.
+STEP_KERNEL_NCU = {"dram_bytes_per_launch": 10.97e6, "warp_inst_per_particle_step": 2.57e9 / 2.4e7,
+                   "particle_steps_per_launch": 2.4e7}
+SM_COUNT, SMSP_PER_SM = 148, 4
 CPU_SAMPLE_STEPS = 40  # outer steps of all particles per step of the reference arm (~5 s on 16 cores)
 CPU_BASELINE_STEPS = 120  # outer steps of all particles in the B200 arm's cpu_baseline sample (one met hour)
 CPU_BASELINE_REPEATS = 3  # the hour stepped this many times (~15 s on 16 cores)
@@ -1048,11 +1055,17 @@ def main() -> None:
                        "autotune_steps_per_launch_ms": {str(k or "window"): round(v, 3)
                                                         for k, v in tuned.get("steps_times_ms", {}).items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         # ncu DRAM bytes of one window's launch (the same workload's launch)
+                         "traffic": STEP_KERNEL_NCU["dram_bytes_per_launch"] if args.met == "f32" else None,
                          "kernel": "step_kernel", "bytes_per_particle_step": B_ALG[args.met],
-                         "kernel_time_share": t_kernel / t_dev},
+                         "kernel_time_share": t_kernel / t_dev,
+                         "limiter": "instruction issue: the plume's met gathers hit L1 (DRAM traffic ~1/2000 of "
+                                    "the algorithmic bytes), so the HBM frac is nominal",
+                         "issue": issue_fraction(p_steps / t_kernel, clk)},
             "clocks": clk,
-            # step launches + 3 per particle-order rebuild + per window: 2 packing, 2 column, 1 redistribution
+            # step launches (the convection fused in) + 3 per particle-order rebuild + per window: 3 packing
+            # (surface, cells, wind sums) and 2 for the convection column
             "gpu_launches": n_kernel_launches + 3 * reorders[0] + 5 * args.steps,
             "status": status,
         }
@@ -1078,6 +1091,18 @@ def main() -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def issue_fraction(kernel_particle_steps_per_s: float, clk: dict) -> dict:
+    """The step kernel's instruction-issue rate against the issue ceiling (one warp
+    instruction per SM sub-partition per clock): warp instructions per particle-step from
+    the ncu capture x the live particle-steps/s, over 148 x 4 x the median SM clock
+    sampled during the timed region."""
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    achieved = STEP_KERNEL_NCU["warp_inst_per_particle_step"] * kernel_particle_steps_per_s
+    peak = SM_COUNT * SMSP_PER_SM * mhz * 1e6
+    return {"achieved_warp_inst_per_s": achieved, "peak_warp_inst_per_s": peak, "frac": achieved / peak,
+            "warp_inst_per_particle_step": STEP_KERNEL_NCU["warp_inst_per_particle_step"], "sm_mhz": mhz}
 
 
 def run_extras(args, syn, cfg, value: float, line: dict) -> dict:
