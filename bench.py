@@ -153,6 +153,13 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.gpu), "-lms", "20"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: the timed region begins once it samples
+            t_end = time.monotonic() + 3.0
+            while time.monotonic() < t_end and self.proc.poll() is None:
+                self.f.flush()
+                if self.path.stat().st_size > 0:
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -1006,9 +1013,13 @@ def main() -> None:
             steps_per_window.append(j1 - j0)
         torch.cuda.synchronize()
         record_kernels = False
-    if world > 1:
-        dist.barrier()
-    t_dev = sum(a.elapsed_time(b) for a, b in win_events) / 1e3
+        if world > 1:
+            dist.barrier()
+        t_dev = sum(a.elapsed_time(b) for a, b in win_events) / 1e3
+        # ---- end to end (met in pinned host memory, copies inside the timed region), sampled too
+        e2e = None
+        if not args.no_e2e:
+            e2e = run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, world)
     t_kernel = sum(a.elapsed_time(b) for a, b in kernel_events) / 1e3
     n_kernel_launches = len(kernel_events)
     out = run.finish() if run.done else None
@@ -1023,10 +1034,6 @@ def main() -> None:
     value = world * p_steps / t_max
     ms_per_step = 1e3 * t_max / args.steps
 
-    # ---- end to end: met in pinned host memory, copies inside the timed region
-    e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(args, cfg, syn, grid, make_runner, fresh_state, kw, dev, stream, world)
 
     # ---- the whole job captured into one CUDA graph, replayed once
     graph = None
