@@ -107,3 +107,24 @@ def test_release_assembler_sums_a_bin_delivered_twice():
         b, c, v = part
         asm2(np.array([7]), np.array([b]), np.array([0, len(c)]), np.array(c, np.int32), np.array(v, np.float32))
     np.testing.assert_array_equal(got[7], np.array([[1.0, 0.0, 2.5], [0.0, 4.0, 0.0]], np.float32))
+
+
+def test_float64_slices_round_trip_and_assemble():
+    """FP64 footprints (``value_f64``): the oracle's compaction keeps float64 values
+    bit-exactly, the package's ``densify`` rebuilds them in float64, and the assembler
+    hands float64 blocks to the writer when built with ``dtype=np.float64``."""
+    from glide_b200.sparse import ReleaseAssembler, densify
+
+    rng = np.random.default_rng(9)
+    shape = (1, 7, 11)
+    x = _slices(rng, 4, shape).astype(np.float64)
+    x.reshape(4, -1)[0, :3] = np.array([5e-324, -0.0, 1.0 + 2.0**-40])  # not representable in float32
+    off, cell, val = osp.compact(x)
+    assert val.dtype == np.float64
+    np.testing.assert_array_equal(osp.densify(off, cell, val, shape).view(np.uint64), x.view(np.uint64))
+    np.testing.assert_array_equal(densify(off, cell, val, shape).view(np.uint64), x.view(np.uint64))
+    got = {}
+    asm = ReleaseAssembler(2, shape, lambda r, block: got.__setitem__(r, block), dtype=np.float64)
+    asm(np.array([3, 3]), np.array([0, 1]), off[:3], cell, val)
+    assert got[3].dtype == np.float64
+    np.testing.assert_array_equal(got[3].reshape(2, -1).view(np.uint64), x[:2].reshape(2, -1).view(np.uint64))
