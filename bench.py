@@ -93,6 +93,8 @@ def parse():
     ap.add_argument("--days", type=float, default=5.0)
     ap.add_argument("--periodic-releases", type=int, default=720,
                     help="periodic: hourly releases of 20,000 particles (the reference's example has 720)")
+    ap.add_argument("--no-diagnostics", action="store_true",
+                    help="skip the per-step mean-position / mean-wind diagnostics (BatchRunner.diagnostics)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload: skip the extra jobs (reference GPU path, multisite, periodic)")
     ap.add_argument("--dense-footprints", action="store_true",
@@ -948,6 +950,7 @@ def main() -> None:
         r.steps_per_launch = tuned["steps_per_launch"]
         r.fuse_convection = not args.separate_convection
         r.reorder = not args.no_reorder
+        r.diagnostics = not args.no_diagnostics
         return r
 
     def fresh_state():
