@@ -21,6 +21,7 @@ GLIDE_STATUS_BAD_ROW, GLIDE_STATUS_COMPACT_OVERFLOW = 4, 8
 GLIDE_WORK_DONE, GLIDE_WORK_PENDING, GLIDE_WORK_CLASSES = 0, 63, 64
 GLIDE_STEP_BATCH_MAX = 32
 GLIDE_REGRID_MAX_LEVELS = 256
+GLIDE_DIAG_DEG_SCALE, GLIDE_DIAG_M_SCALE = 1 << 20, 1 << 10
 
 vp = C.c_void_p
 
@@ -64,7 +65,7 @@ class StepArgs(C.Structure):
                 ("dom_lat_min", C.c_double), ("dom_lat_max", C.c_double), ("dom_alt_max", C.c_double),
                 ("escaped_per_step", vp), ("active_per_step", vp), ("status", vp), ("launch_variant", C.c_int32),
                 ("order", vp), ("work_key", vp), ("conv_column", vp), ("conv_step", C.c_int32),
-                ("conv_nz", C.c_int32), ("conv_uniforms", vp), ("conv_moved", vp), ("diag_pos_sum", vp)]
+                ("conv_nz", C.c_int32), ("conv_uniforms", vp), ("conv_moved", vp), ("diag_pos_fixed", vp)]
 
 
 class ConvectArgs(C.Structure):

@@ -64,22 +64,39 @@ struct StepDev {
     uint32_t* status;
     const int32_t* order; uint8_t* work_key;
     const double* conv_column; int conv_step, conv_nz; const float* conv_uniforms; int32_t* conv_moved;
-    double* diag;
+    long long* diag;
 };
 
 // Dynamic shared memory of one block: when the launch sums the position diagnostic,
-// [3] float64 position sums of the block's idle warps (constant over the launch) and
-// [n_steps][3] float64 position sums of the others; then [2][n_steps] int32 escaped /
-// active counts.
+// [3] fixed-point position sums of the block's idle warps (constant over the launch)
+// and [n_steps][3] fixed-point position sums of the others; then [2][n_steps] int32
+// escaped / active counts.
 __host__ __device__ inline size_t step_smem_bytes(int n_steps, bool diag) {
-    return (diag ? sizeof(double) * 3 * (size_t)(n_steps + 1) : 0) + sizeof(int32_t) * 2 * (size_t)n_steps;
+    return (diag ? sizeof(long long) * 3 * (size_t)(n_steps + 1) : 0) + sizeof(int32_t) * 2 * (size_t)n_steps;
 }
 
-// Sum of v over the 32 lanes of a converged warp, in every lane.
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+// Sum over the 32 lanes of a converged warp of v quantised to 1 / scale (v * scale,
+// scale a power of two, rounded to the nearest integer; |v * scale| < 2^31), exactly:
+// the quantised values' high and low bits summed by two integer warp reductions.
+// Integer sums do not depend on the order of the additions, so the diagnostic is the
+// same from run to run and for any launch shape or particle order.
+__device__ __forceinline__ long long warp_sum_fixed(float v, float scale) {
+    const int q = __float2int_rn(v * scale);
+    const int hi = __reduce_add_sync(0xffffffffu, q >> 12);  // floor(q / 4096): |hi| < 2^19, sum < 2^24
+    const unsigned lo = __reduce_add_sync(0xffffffffu, (unsigned)(q & 0xfff));
+    return ((long long)hi << 12) + (long long)lo;
+}
+
+// The three position sums of a warp (lanes without a particle add zero).
+__device__ __forceinline__ void warp_position_sums(bool have, float lon, float lat, float z, long long* dst) {
+    const long long sx = warp_sum_fixed(have ? lon : 0.0f, (float)GLIDE_DIAG_DEG_SCALE);
+    const long long sy = warp_sum_fixed(have ? lat : 0.0f, (float)GLIDE_DIAG_DEG_SCALE);
+    const long long sz = warp_sum_fixed(have ? z : 0.0f, (float)GLIDE_DIAG_M_SCALE);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(dst), (unsigned long long)sx);
+        atomicAdd(reinterpret_cast<unsigned long long*>(dst + 1), (unsigned long long)sy);
+        atomicAdd(reinterpret_cast<unsigned long long*>(dst + 2), (unsigned long long)sz);
+    }
 }
 
 // Smallest and largest cursor offset of the launch's steps, in every lane of the warp.
@@ -319,9 +336,9 @@ constexpr int kNumVariants = kNumShapes + 1;
 // The whole launch body for one batch; `block` is the block's index within the batch.
 template <typename T, bool GENERAL>
 __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
-    extern __shared__ double s_dyn[];
-    double* const s_static = s_dyn;     // [3] when p.diag
-    double* const s_diag = s_dyn + 3;   // [n_steps][3] when p.diag
+    extern __shared__ long long s_dyn[];
+    long long* const s_static = s_dyn;     // [3] when p.diag
+    long long* const s_diag = s_dyn + 3;   // [n_steps][3] when p.diag
     int32_t* const s_counts = reinterpret_cast<int32_t*>(s_dyn + (p.diag ? 3 * (p.n_steps + 1) : 0));  // [2][n_steps]
     const int64_t th = block * blockDim.x + threadIdx.x;
     bool have = th < p.n;
@@ -335,7 +352,7 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
     const int lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < 2 * p.n_steps; k += blockDim.x) s_counts[k] = 0;
     if (p.diag)
-        for (int k = threadIdx.x; k < 3 * (p.n_steps + 1); k += blockDim.x) s_dyn[k] = 0.0;
+        for (int k = threadIdx.x; k < 3 * (p.n_steps + 1); k += blockDim.x) s_dyn[k] = 0;
     __syncthreads();
 
     float lon = 0.f, lat = 0.f, z = 0.f, wgt = 0.f, up = 0.f, vp = 0.f, wp = 0.f, um = 0.f, vm = 0.f;
@@ -379,16 +396,7 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
         idle_warp = __all_sync(0xffffffffu, idle);
     }
     if (idle_warp) {
-        if (p.diag) {
-            const double sx = warp_sum(have ? (double)lon : 0.0);
-            const double sy = warp_sum(have ? (double)lat : 0.0);
-            const double sz = warp_sum(have ? (double)z : 0.0);
-            if (lane == 0) {
-                atomicAdd(&s_static[0], sx);
-                atomicAdd(&s_static[1], sy);
-                atomicAdd(&s_static[2], sz);
-            }
-        }
+        if (p.diag) warp_position_sums(have, lon, lat, z, s_static);
         if (have && p.work_key) {
             const glide_step_sched sl = p.sched ? p.sched[p.n_steps - 1] : p.sched0;
             p.work_key[i] = (uint8_t)((alive && !(rel >= sl.cursor_off)) ? GLIDE_WORK_PENDING : GLIDE_WORK_DONE);
@@ -647,16 +655,7 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
                     if (n_act) atomicAdd(&s_counts[p.n_steps + j], n_act);
                 }
                 // --- mean-position diagnostic (main.py:1565-1566): sums over every particle
-                if (p.diag) {
-                    const double sx = warp_sum(have ? (double)lon : 0.0);
-                    const double sy = warp_sum(have ? (double)lat : 0.0);
-                    const double sz = warp_sum(have ? (double)z : 0.0);
-                    if (lane == 0) {
-                        atomicAdd(&s_diag[3 * j], sx);
-                        atomicAdd(&s_diag[3 * j + 1], sy);
-                        atomicAdd(&s_diag[3 * j + 2], sz);
-                    }
-                }
+                if (p.diag) warp_position_sums(have, lon, lat, z, s_diag + 3 * j);
             }
         }
 
@@ -690,7 +689,8 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
     }
     if (p.diag)
         for (int k = threadIdx.x + p.post_begin * 3; k < 3 * p.n_steps; k += blockDim.x)
-            atomicAdd(p.diag + k, s_diag[k] + s_static[k % 3]);
+            atomicAdd(reinterpret_cast<unsigned long long*>(p.diag + k),
+                      (unsigned long long)(s_diag[k] + s_static[k % 3]));
 }
 
 template <typename T, int THREADS, int MIN_BLOCKS, bool GENERAL>
@@ -728,7 +728,7 @@ static glide_status launch_step(const StepDev& d, cudaStream_t stream, int varia
     const size_t smem = step_smem_bytes(d.n_steps, d.diag != nullptr);
     if (smem > 48 * 1024)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: n_steps %d too large%s", d.n_steps,
-                         d.diag ? " with diag_pos_sum (at most 1535)" : "");
+                         d.diag ? " with diag_pos_fixed (at most 1535)" : "");
     switch (variant) {
         case 0: launch_shape<T, 0, false>(d, stream, smem); break;
         case 1: launch_shape<T, 1, false>(d, stream, smem); break;
@@ -769,8 +769,8 @@ static glide_status validate_step(const glide_step_args* a) {
     if (a->max_substeps < 1) return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: max_substeps < 1");
     if (a->phys_begin < 0 || a->post_begin < 0)
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: phys_begin / post_begin < 0");
-    if (a->diag_pos_sum && ((uintptr_t)a->diag_pos_sum & 7u))
-        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: diag_pos_sum must be 8-byte aligned");
+    if (a->diag_pos_fixed && ((uintptr_t)a->diag_pos_fixed & 7u))
+        return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: diag_pos_fixed must be 8-byte aligned");
     if (a->footprint && a->fp.value_f64 && ((uintptr_t)a->footprint & 7u))
         return set_error(GLIDE_ERR_INVALID_ARG, "glide_step: a float64 footprint must be 8-byte aligned");
     if (a->launch_variant < 0 || a->launch_variant >= kNumVariants)
@@ -828,7 +828,7 @@ static StepDev make_step_dev(const glide_step_args* a) {
     d.order = a->order; d.work_key = a->work_key;
     d.conv_column = static_cast<const double*>(a->conv_column); d.conv_step = a->conv_step; d.conv_nz = a->conv_nz;
     d.conv_uniforms = a->conv_uniforms; d.conv_moved = a->conv_moved;
-    d.diag = a->diag_pos_sum;
+    d.diag = reinterpret_cast<long long*>(a->diag_pos_fixed);
     return d;
 }
 

@@ -261,10 +261,10 @@ class BatchRun:
         self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        # per-step diagnostics: position sums [n_steps][3] (the step kernel adds to them) and
-        # each window's wind sums [n_windows][6] (copied from its packed window)
+        # per-step diagnostics: fixed-point position sums [n_steps][3] (the step kernel adds to
+        # them) and each window's wind sums [n_windows][6] (copied from its packed window)
         self.diagnostics = runner.diagnostics
-        self.diag_sum = torch.zeros((max(1, len(steps)), 3), dtype=torch.float64, device=dev) \
+        self.diag_sum = torch.zeros((max(1, len(steps)), 3), dtype=torch.int64, device=dev) \
             if self.diagnostics else None
         fp = runner.footprint
         self.footprint = torch.zeros(fp.device_shape, dtype=fp.torch_dtype, device=dev)
@@ -370,7 +370,7 @@ class BatchRun:
         a.escaped_per_step = self.esc.data_ptr() + 4 * j0
         a.active_per_step = self.act.data_ptr() + 4 * j0
         a.status = self.status.data_ptr()
-        a.diag_pos_sum = None if self.diag_sum is None else self.diag_sum.data_ptr() + 24 * j0
+        a.diag_pos_fixed = None if self.diag_sum is None else self.diag_sum.data_ptr() + 24 * j0
         a.launch_variant = r.launch_variant
         if self.work_key is not None:
             a.order = self.order.data_ptr() if self.order_valid else None
@@ -689,7 +689,10 @@ class BatchRun:
         out = BatchOutput(self.state, fp, self.esc[:n].cpu().numpy(), self.act[:n].cpu().numpy(), n,
                           self.conv_log, status)
         if self.diag_sum is not None and n > 0:
-            out.diag_pos = (self.diag_sum[:n].cpu().numpy() / max(1, self.state.n)).astype(np.float32)
+            scale = np.array([_abi.GLIDE_DIAG_DEG_SCALE, _abi.GLIDE_DIAG_DEG_SCALE, _abi.GLIDE_DIAG_M_SCALE],
+                             dtype=np.float64)
+            sums = self.diag_sum[:n].cpu().numpy().astype(np.float64) / scale
+            out.diag_pos = (sums / max(1, self.state.n)).astype(np.float32)
             out.diag_wind = self._diag_wind(self.wind_sum.cpu().numpy())
         return out
 

@@ -28,6 +28,10 @@ enum {
     GLIDE_ERR_UNSUPPORTED = 3,
 };
 
+/* fixed-point scales of glide_step_args.diag_pos_fixed (2^20 per degree, 2^10 per metre) */
+#define GLIDE_DIAG_DEG_SCALE 1048576
+#define GLIDE_DIAG_M_SCALE 1024
+
 /* storage type of the packed met bricks */
 enum { GLIDE_MET_F32 = 0, GLIDE_MET_BF16 = 1, GLIDE_MET_F16 = 2 };
 
@@ -177,12 +181,15 @@ typedef struct glide_step_args {
     const void* conv_column; int32_t conv_step; int32_t conv_nz;
     const float* conv_uniforms;   /* injected uniforms [2][n], or NULL: Philox keyed by seed */
     int32_t* conv_moved;          /* device counter of moved particles (added to), may be NULL */
-    /* optional per-step diagnostic, device [n_steps][3] float64 (added to; NULL = none): the
-     * sums of lon, lat and z over all n particles (active or not) after each step's
-     * post-step; divided by n they are the runtime's mean-position diagnostic
-     * (particles[:, :3].mean(0), src/lpdm/main.py:1565-1566). Only steps j >= post_begin
-     * are summed; n_steps is then at most 1535. */
-    double* diag_pos_sum;
+    /* optional per-step diagnostic, device [n_steps][3] int64 (added to; NULL = none): the
+     * sums over all n particles (active or not), after each step's post-step, of lon and
+     * lat quantised to 1 / GLIDE_DIAG_DEG_SCALE degree and z to 1 / GLIDE_DIAG_M_SCALE m
+     * (each value times the scale, rounded to the nearest integer). Divided by the scale
+     * and n they are the runtime's mean-position diagnostic (particles[:, :3].mean(0),
+     * src/lpdm/main.py:1565-1566). Integer sums: the result does not depend on the
+     * launch shape or the particle order. Only steps j >= post_begin are summed; n_steps
+     * is then at most 1535. Positions must stay below 2048 degrees and 2097 km. */
+    int64_t* diag_pos_fixed;
 } glide_step_args;
 
 /* Emanuel convection for one window (src/lpdm/convection/emanuel.py:570-805). */

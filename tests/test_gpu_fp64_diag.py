@@ -169,7 +169,7 @@ def test_diagnostics_match_reference(cuda_device, name):
     assert pos.max() < (1e-6 if name == "run_c1" else 5e-3), pos.max()
     parts, _, _, _ = as_numpy(out)
     own = parts[:3].astype(np.float64).mean(axis=1).astype(np.float32)
-    np.testing.assert_allclose(out.diag_pos[-1], own, rtol=2e-7)
+    np.testing.assert_allclose(out.diag_pos[-1], own, rtol=1e-6)  # sums of positions quantised to 2^-20 deg, 2^-10 m
     rows = out.diagnostic_rows()
     assert len(rows) == out.n_steps and rows[-1]["alive_particles"] == int(out.state.alive.sum().item())
 
