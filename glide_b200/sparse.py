@@ -99,8 +99,9 @@ class SparseSliceStream:
     Per call (one window's completed (release, bin) slices): ``glide_footprint_compact`` on
     the step stream reads the slices straight from the ring rows and clears them (the
     ring slot is free for a later bin in stream order); on ``copy_stream`` the slice
-    offsets and a speculative prefix of the entries (``headroom`` x the densest slice
-    seen so far, per slice) go to pinned host memory. When the call's buffer is needed
+    offsets and a speculative prefix of the entries (``headroom`` x the call's slices x
+    the expected entries per slice: a maximum of the recent calls' mean entries per slice
+    that decays by ``decay`` per call) go to pinned host memory. When the call's buffer is needed
     again (or at ``drain()``) the host waits for those copies, copies whatever the
     speculation missed, and calls ``on_host(r_idx, b_idx, slice_offset, cell, value)``
     (numpy arrays, valid during the call). The device buffers are sized for every
@@ -108,12 +109,14 @@ class SparseSliceStream:
     the compaction never overflows; ``capacity`` sizes them for that many slices up
     front.
 
-    ``bytes_moved`` counts the bytes copied to the host; ``dense_bytes`` what the dense
-    slices would have been. ``dtype`` is the footprint's value type (float32 or float64)."""
+    ``bytes_moved`` counts the bytes copied to the host (``speculated`` the entries of the
+    speculative copies, ``short_copies`` the calls whose speculation was short and took a
+    second copy); ``dense_bytes`` what the dense slices would have been. ``dtype`` is the
+    footprint's value type (float32 or float64)."""
 
     def __init__(self, device, slice_shape: tuple, on_host: Callable | None = None, buffers: int = 2,
                  headroom: float = 1.25, initial_density: float = 1.0 / 32.0, capacity: int = 0,
-                 dtype: torch.dtype = torch.float32) -> None:
+                 dtype: torch.dtype = torch.float32, decay: float = 0.95) -> None:
         self.device = torch.device(device)
         self.dtype = dtype
         self.value_bytes = torch.empty((), dtype=dtype).element_size()
@@ -122,6 +125,8 @@ class SparseSliceStream:
         self.on_host = on_host
         self.headroom = float(headroom)
         self.per_slice = float(initial_density) * self.cells  # speculation: entries per slice
+        self.decay = float(decay)
+        self.speculated = 0
         self.copy_stream = torch.cuda.Stream(device=self.device)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.slots = [{"k": 0, "h": 0} for _ in range(max(1, int(buffers)))]
@@ -179,8 +184,8 @@ class SparseSliceStream:
                 ev = self.copy_stream.record_event()
             ev.synchronize()
             self.bytes_moved += (total - spec) * (4 + self.value_bytes)
-        if k > 0:
-            self.per_slice = max(self.per_slice, float(np.diff(off).max()))
+        if k > 0:  # a call's slices average out: follow their mean density, forget old peaks slowly
+            self.per_slice = max(self.per_slice * self.decay, total / k)
         self.entries += total
         if self.on_host is not None:
             idx = slot["h_idx"][:, :k].numpy()
@@ -202,6 +207,7 @@ class SparseSliceStream:
         compact_rows(rows, flat, clear=clear, capacity=k * self.cells, status=self.status,
                      out=(slot["off"], slot["cell"], slot["value"]), scratch=slot["scratch"], stream=cur)
         spec = min(k * self.cells, int(np.ceil(self.headroom * self.per_slice * k)))
+        self.speculated += spec
         self._host_entries(slot, spec)
         ready = cur.record_event()
         with torch.cuda.stream(self.copy_stream):
