@@ -761,6 +761,9 @@ class HostSliceStream:
             self.on_host(idx[0].copy(), idx[1].copy(), buf["slices"][:k])
 
     def __call__(self, r_idx: torch.Tensor, b_idx: torch.Tensor, slices: torch.Tensor) -> None:
+        if slices.dtype != self.dtype:
+            raise ValueError(f"HostSliceStream holds {self.dtype} slices, got {slices.dtype} "
+                             "(pass dtype= to match the footprint's value type)")
         k = int(slices.shape[0])
         slot = self.next
         self.next = (self.next + 1) % len(self.bufs)
