@@ -1,13 +1,14 @@
 // Particle ordering by work class: a stable counting sort of particle indices by
 // the work key the step kernel writes (glide_step_args.work_key), descending.
 //
-// The step kernel runs one particle per thread and a per-particle number of
-// exact-OU substeps (1 .. max_substeps): a warp runs as many substeps as its
-// busiest lane. Grouping particles of equal substep count into the same warps
-// (and escaped particles into warps that exit at once) removes that idle-lane
-// time; ordering heavy classes first starts the longest blocks first. The
-// sort is stable within a class so that neighbouring particles (same release,
-// nearby met cells) stay neighbours.
+// The step kernel runs one particle per thread, and a particle's path through a
+// step (substep count, stability regime, closure branch, boundary layer or free
+// troposphere) follows its height relative to the boundary-layer top: a warp runs
+// every path one of its lanes takes. Grouping particles of one class (substeps x
+// height band x regime) into the same warps, and escaped particles into warps that
+// exit at once, removes that idle-lane time; ordering classes descending puts
+// pending particles first. The sort is stable within a class so that neighbouring
+// particles (same release, nearby met cells) stay neighbours.
 //
 //   tile_hist     per 1024-particle tile, counts per class -> hist[class][tile]
 //   scan_offsets  one block: exclusive scan of hist in class-major order

@@ -530,69 +530,69 @@ __device__ __forceinline__ void step_body(const StepDev& p, int64_t block) {
                 int k = (kq >= (float)ms) ? ms : ((kq >= 1.0f) ? (int)kq : 1);
                 if (!(kq == kq)) k = 1;  // NaN
                 const float sub_dt = delta / (float)k;
-                // work class of this step (glide_step_args.work_key): the closure branch, whether
-                // the free-troposphere override applies, the substep count
-                last_k = 1 + (min(k, 6) - 1) + 6 * ((z_eval > S.blh ? 1 : 0) + 2 * col.branch);
+                // work class of this step (glide_step_args.work_key): the stability regime, the
+                // height band of z_eval within (or above) the BL and the substep count. Height
+                // bands rather than the closure's branches: a particle's branch and its BL/FT
+                // side follow its height relative to the BL top, which drifts within a window,
+                // so warps built from neighbouring bands stay converged longer
+                {
+                    const float hr = z_eval / S.blh;
+                    const int band = hr < 0.25f ? 0 : (hr < 0.5f ? 1 : (hr < 0.8f ? 2 : (hr <= 1.0f ? 3 : 4)));
+                    const int regime = S.hL > 1.0f ? 0 : (S.hL < -1.0f ? 2 : 1);
+                    last_k = 1 + (min(k, 3) - 1) + 3 * (band + 5 * regime);
+                }
 
-                // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507), then
-                // the meander (hanna.py:1028-1054), in one rolled loop: iterations 0 .. k-1 are
-                // the substeps, iteration k (meander on) the meander step. Both end in the same
-                // horizontal displacement, so the kernel holds one copy of it (and of its cos)
-                // and one of the normal draw; the draws keep their order, three per substep
-                // and then two. Lanes of a warp with different substep counts run their meander
-                // steps together with the other lanes' last substeps.
+                // --- exact-OU substeps (hanna.py:1224-1368, gpu_engine.py:26-42, 400-507)
                 const float su2 = su * su, sv2 = sv * sv, sw2 = sw * sw;
                 const float umax = 4.0f * su, vmax = 4.0f * sv, wmax = 4.0f * sw;
                 const float au = ou_decay(sub_dt, tlu), av = ou_decay(sub_dt, tlv), aw = ou_decay(sub_dt, tlw);
                 const float ru = ou_amplitude(su2, au), rv = ou_amplitude(sv2, av), rw = ou_amplitude(sw2, aw);
                 const int64_t nn = p.n;
                 StepNormals rng((uint64_t)i, (uint32_t)sc.step_index, p.seed_lo, p.seed_hi);
-                const int n_it = k + (p.meander ? 1 : 0);
-                for (int it = 0; it < n_it; ++it) {
-                    const bool mea = it == k;
-                    float e0 = 0.f, e1 = 0.f, e2 = 0.f;
-                    const float* nb = GENERAL ? (mea ? p.noise_mea : p.noise_sub) : nullptr;
-                    if (GENERAL && nb) {
-                        const float* b = mea ? nb + ((int64_t)j * 2) * nn + i : nb + ((int64_t)(j * ms + it) * 3) * nn + i;
+                for (int it = 0; it < k; ++it) {
+                    float eu, ev, ew;
+                    if (GENERAL && p.noise_sub) {
+                        const float* b = p.noise_sub + ((int64_t)(j * ms + it) * 3) * nn + i;
+                        eu = __ldg(b);
+                        ev = __ldg(b + nn);
+                        ew = __ldg(b + 2 * nn);
+                    } else {
+                        eu = rng.next();
+                        ev = rng.next();
+                        ew = rng.next();
+                    }
+                    const float factor = 1.0f + (wp * wp) / sw_sq;
+                    const float drift_w = factor * half_bwd + dens_bwd;
+                    float un = ou_step(up, au, 0.0f * sub_dt, ru, eu);
+                    float vn = ou_step(vp, av, 0.0f * sub_dt, rv, ev);
+                    float wn = ou_step(wp, aw, drift_w * sub_dt, rw, ew);
+                    wn = fminf(fmaxf(wn, -wmax), wmax);
+                    un = fminf(fmaxf(un, -umax), umax);
+                    vn = fminf(fmaxf(vn, -vmax), vmax);
+                    z = displace_z(z, wn, sub_dt, -1.0f);
+                    lon = displace_lon(lon, un, sub_dt, -1.0f, m_per_deg_lon(lat));
+                    lat = displace_lat(lat, vn, sub_dt, -1.0f);
+                    reflect_surface(z, wn, 0.0f);
+                    up = un; vp = vn; wp = wn;
+                }
+
+                // --- meander (hanna.py:1028-1054)
+                if (p.meander) {
+                    float e0, e1;
+                    if (GENERAL && p.noise_mea) {
+                        const float* b = p.noise_mea + ((int64_t)j * 2) * nn + i;
                         e0 = __ldg(b);
                         e1 = __ldg(b + nn);
-                        if (!mea) e2 = __ldg(b + 2 * nn);
                     } else {
-                        const int nd = mea ? 2 : 3;
-#pragma unroll 1
-                        for (int d = 0; d < nd; ++d) {
-                            const float v = rng.next();
-                            e0 = d == 0 ? v : e0;
-                            e1 = d == 1 ? v : e1;
-                            e2 = d == 2 ? v : e2;
-                        }
+                        e0 = rng.next();
+                        e1 = rng.next();
                     }
-                    float un, vn, dt, wn = 0.f;
-                    if (!mea) {
-                        const float factor = 1.0f + (wp * wp) / sw_sq;
-                        const float drift_w = factor * half_bwd + dens_bwd;
-                        un = ou_step(up, au, 0.0f * sub_dt, ru, e0);
-                        vn = ou_step(vp, av, 0.0f * sub_dt, rv, e1);
-                        wn = ou_step(wp, aw, drift_w * sub_dt, rw, e2);
-                        wn = fminf(fmaxf(wn, -wmax), wmax);
-                        un = fminf(fmaxf(un, -umax), umax);
-                        vn = fminf(fmaxf(vn, -vmax), vmax);
-                        z = displace_z(z, wn, sub_dt, -1.0f);
-                        dt = sub_dt;
-                    } else {
-                        const float am = ou_decay(delta, p.meander_T);
-                        un = ou_step(um, am, 0.0f * delta, ou_amplitude(m_su * m_su, am), e0);
-                        vn = ou_step(vm, am, 0.0f * delta, ou_amplitude(m_sv * m_sv, am), e1);
-                        dt = delta;
-                    }
-                    lon = displace_lon(lon, un, dt, -1.0f, m_per_deg_lon(lat));
-                    lat = displace_lat(lat, vn, dt, -1.0f);
-                    if (!mea) {
-                        reflect_surface(z, wn, 0.0f);
-                        up = un; vp = vn; wp = wn;
-                    } else {
-                        um = un; vm = vn;
-                    }
+                    const float am = ou_decay(delta, p.meander_T);
+                    const float umn = ou_step(um, am, 0.0f * delta, ou_amplitude(m_su * m_su, am), e0);
+                    const float vmn = ou_step(vm, am, 0.0f * delta, ou_amplitude(m_sv * m_sv, am), e1);
+                    lon = displace_lon(lon, umn, delta, -1.0f, m_per_deg_lon(lat));
+                    lat = displace_lat(lat, vmn, delta, -1.0f);
+                    um = umn; vm = vmn;
                 }
                 nonfinite |= !(isfinite(lon) && isfinite(lat) && isfinite(z) && isfinite(up) && isfinite(vp) &&
                                isfinite(wp));

@@ -44,9 +44,10 @@ enum {
 };
 
 /* work classes written to glide_step_args.work_key: GLIDE_WORK_DONE, GLIDE_WORK_PENDING, or
- * for a particle stepped in the launch's last step 1 + (min(k, 6) - 1) + 6 (ft + 2 branch),
- * k its substeps, ft 1 above the boundary layer, branch the Hanna closure branch (0 stable,
- * 1 neutral, 2-4 the unstable T_Lw forms): classes 1 .. 60 */
+ * for a particle stepped in the launch's last step 1 + (min(k, 3) - 1) + 3 (band + 5 regime),
+ * k its substeps, band the height band of z_eval / boundary-layer height (0: below 0.25,
+ * 1: below 0.5, 2: below 0.8, 3: at most 1, 4: above the boundary layer), regime the
+ * stability regime (0 stable h/L > 1, 1 neutral, 2 unstable h/L < -1): classes 1 .. 45 */
 enum { GLIDE_WORK_DONE = 0, GLIDE_WORK_PENDING = 63, GLIDE_WORK_CLASSES = 64 };
 
 /* Met grid geometry: GridInterpolationBounds (src/lpdm/gpu_engine.py:100-121). */

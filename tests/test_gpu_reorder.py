@@ -112,8 +112,9 @@ def test_steps_per_launch_gives_the_same_results(cuda_device, name, injected):
 
 
 def test_work_keys_and_bad_order(cuda_device):
-    """The work keys a window writes: DONE for escaped particles, 1..max_substeps or
-    PENDING for live ones; an order entry outside [0, n) is skipped and flagged."""
+    """The work keys a window writes: DONE for escaped particles, a class 1..45 (substeps
+    x height band x stability regime) or PENDING for live ones; an order entry outside
+    [0, n) is skipped and flagged."""
     from glide_b200 import _abi
     from glide_b200.runtime import stream_handle
     from gpu_cases import runner_for, state_from
@@ -132,12 +133,15 @@ def test_work_keys_and_bad_order(cuda_device):
     ms = int(z["max_substeps"])
     assert np.all(keys[~alive] == _abi.GLIDE_WORK_DONE)
     live = keys[alive].astype(np.int64)
-    stepped = (live >= 1) & (live <= 60)
+    stepped = (live >= 1) & (live <= 45)
     assert np.all(stepped | (live == _abi.GLIDE_WORK_PENDING))
     assert np.any(stepped)
-    k = (live[stepped] - 1) % 6 + 1  # substeps (capped at 6)
-    branch = (live[stepped] - 1) // 12
-    assert np.all(k <= ms) and np.all(branch <= 4)
+    cls = live[stepped] - 1
+    k = cls % 3 + 1  # substeps (capped at 3)
+    band = (cls // 3) % 5  # height band relative to the BL top
+    regime = cls // 15  # stable / neutral / unstable
+    assert np.all(k <= min(ms, 3)) and np.all(band <= 4) and np.all(regime <= 2)
+    assert len(np.unique(band)) > 1  # the batch spans several height bands
 
     # one single-step launch of the next window through a corrupted permutation
     k = br.next_window
