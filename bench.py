@@ -50,7 +50,7 @@ METRIC = "particle-steps/s"
 # the release, 200,000 particles x 120 steps; profiles/step_kernel_single_site_f32.md):
 # DRAM bytes per launch and warp instructions issued per particle-step. The plume's met
 # is served from L1, so the kernel is bound by instruction issue, not by HBM.
-STEP_KERNEL_NCU = {"dram_bytes_per_launch": 10.98e6, "warp_inst_per_particle_step": 2.649e9 / 2.4e7,
+STEP_KERNEL_NCU = {"dram_bytes_per_launch": 10.998e6, "warp_inst_per_particle_step": 2.599e9 / 2.4e7,
                    "particle_steps_per_launch": 2.4e7}
 SM_COUNT, SMSP_PER_SM = 148, 4
 CPU_SAMPLE_STEPS = 40  # outer steps of all particles per step of the reference arm (~5 s on 16 cores)
