@@ -43,16 +43,12 @@ __device__ inline double theta(double t, double p) { return t * pow(P0 / fmax(p,
 __device__ inline double theta_e(double t, double q, double p) {
     return theta(t, p) * exp(LV * q / (CP * fmax(t_lcl_bolton(t, q, p), T_MIN)));
 }
-__device__ inline double lift_moist(double te, double p) {  // fixed 30-step bisection in [180, 350] K
-    double lo = 180.0, hi = 350.0;
-    for (int it = 0; it < 30; ++it) {
-        const double mid = 0.5 * (lo + hi);
-        const double qs = e_to_q(e_sat(mid), p);
-        if (theta_e(mid, qs, p) > te) hi = mid; else lo = mid;
-    }
-    return 0.5 * (lo + hi);
-}
 }  // namespace conv
+
+// Lanes per level of the parcel lift's parallel bisection (a power of two dividing 32;
+// eight lanes resolve three bisection steps per round, ten rounds the thirty steps).
+constexpr int kLiftLanes = 8;
+constexpr int kBuildThreads = 512;
 
 struct ConvDev {
     int64_t n;
@@ -100,16 +96,27 @@ __global__ void column_reduce_kernel(const ConvDev d) {
     }
 }
 
-// One block of >= nz threads; shared arrays sized by the launch (dynamic smem).
-__global__ void column_build_kernel(const ConvDev d) {
+// Dynamic shared memory of the column build: ten per-level arrays, and the nz x nz
+// matrix too when the whole fits the default 48 KB (nz <= 73); a larger matrix is
+// built in the scratch buffer itself.
+__host__ inline bool column_matrix_in_smem(int nz) { return sizeof(double) * (10 * (size_t)nz + (size_t)nz * nz) <= 48 * 1024; }
+__host__ inline size_t column_build_smem(int nz) {
+    return sizeof(double) * (10 * (size_t)nz + (column_matrix_in_smem(nz) ? (size_t)nz * nz : 0));
+}
+
+// One block of kBuildThreads threads; shared arrays sized by the launch (dynamic smem). The
+// matrix is built in shared memory when the launch provides room for it (the
+// per-row passes then read shared instead of global memory) and copied to the
+// scratch buffer at the end.
+__global__ void __launch_bounds__(kBuildThreads) column_build_kernel(const ConvDev d, int matrix_in_smem) {
     const int n = d.nz;
     extern __shared__ double sm[];
     double* T = sm;            // ascending-ordered columns
     double* Q = T + n;
     double* P = Q + n;
     double* H = P + n;
-    double* TP = H + n;        // parcel temperature
-    double* TVE = TP + n;      // tv env
+    double* LP = H + n;        // log of the (floored) pressure
+    double* TVE = LP + n;      // tv env
     double* TVP = TVE + n;     // tv parcel
     double* M = TVP + n;       // layer mass
     double* E = M + n;         // entrainment
@@ -117,7 +124,8 @@ __global__ void column_build_kernel(const ConvDev d) {
     __shared__ double s_plcl, s_te, s_thsfc, s_scale;
     __shared__ int s_fires, s_ilcl, s_ilnb;
     double* S = d.scratch;
-    double* cum = S + 8 + 4 * n;
+    double* const cum_out = S + 8 + 4 * n;
+    double* const cum = matrix_in_smem ? D + n : cum_out;
     const int tid = threadIdx.x;
     const bool asc = S[8 + 2 * n + (n - 1)] > S[8 + 2 * n];
     for (int k = tid; k < n; k += blockDim.x) {
@@ -136,14 +144,46 @@ __global__ void column_build_kernel(const ConvDev d) {
         s_thsfc = conv::theta(t0, p0);
     }
     __syncthreads();
-    for (int k = tid; k < n; k += blockDim.x) {  // parcel lift per level (emanuel.py:343-359)
-        const bool below = P[k] >= s_plcl;
-        const double dry = s_thsfc * pow(P[k] / conv::P0, conv::KAPPA);
-        const double tp = below ? dry : conv::lift_moist(s_te, P[k]);
-        TP[k] = tp;
-        TVE[k] = conv::tv(T[k], Q[k]);
-        const double qp = below ? Q[0] : conv::e_to_q(conv::e_sat(tp), P[k]);
-        TVP[k] = conv::tv(tp, qp);
+    // parcel lift per level (emanuel.py:343-359). A moist level's temperature solves
+    // theta_e(T, q_sat(T, p), p) = theta_e of the surface parcel by a fixed 30-step
+    // bisection in [180, 350] K (the temperature returned is the final bracket's
+    // midpoint), run here as ten rounds of an eight-way
+    // split: the eight lanes of a level evaluate the seven interior points of its
+    // bracket at once (exactly the midpoints the bisection can visit in its next
+    // three steps: dyadic points of [180, 350] K, exact in FP64), then every lane
+    // replays the bisection's three steps on those results, so the bracket, and the
+    // temperature, are the serial bisection's bit for bit in a tenth of its latency.
+    for (int base = 0; base < n; base += (int)blockDim.x / kLiftLanes) {  // block-uniform trip count
+        const int k = base + tid / kLiftLanes, sub = tid % kLiftLanes;
+        const bool valid = k < n;
+        const double pk = valid ? P[k] : P[0];
+        double lo = 180.0, hi = 350.0;
+        for (int round = 0; round < 10; ++round) {
+            const double w = hi - lo;
+            bool above = false;
+            if (sub > 0) {
+                const double x = lo + w * (double)sub / (double)kLiftLanes;
+                above = conv::theta_e(x, conv::e_to_q(conv::e_sat(x), pk), pk) > s_te;
+            }
+            const unsigned bits = __ballot_sync(0xffffffffu, above) >> ((tid & 31) & ~(kLiftLanes - 1));
+            int i_lo = 0, i_hi = kLiftLanes;
+            for (int step = 0; step < 3; ++step) {
+                const int mid = (i_lo + i_hi) >> 1;
+                if ((bits >> mid) & 1u) i_hi = mid; else i_lo = mid;
+            }
+            const double nlo = lo + w * (double)i_lo / (double)kLiftLanes;
+            hi = lo + w * (double)i_hi / (double)kLiftLanes;
+            lo = nlo;
+        }
+        if (valid && sub == 0) {
+            const bool below = P[k] >= s_plcl;
+            const double dry = s_thsfc * pow(P[k] / conv::P0, conv::KAPPA);
+            const double tp = below ? dry : 0.5 * (lo + hi);
+            LP[k] = log(fmax(P[k], conv::P_MIN));
+            TVE[k] = conv::tv(T[k], Q[k]);
+            const double qp = below ? Q[0] : conv::e_to_q(conv::e_sat(tp), P[k]);
+            TVP[k] = conv::tv(tp, qp);
+        }
     }
     __syncthreads();
     if (tid == 0) {
@@ -155,8 +195,7 @@ __global__ void column_build_kernel(const ConvDev d) {
         if (i_lcl >= 0) {  // emanuel.py:370-397
             for (int k = 1; k < n; ++k) {
                 const double buoy = (TVP[k] - TVE[k]) / fmax(TVE[k], conv::T_MIN);
-                const double dz = conv::RD * 0.5 * (T[k - 1] + T[k]) *
-                                  (log(fmax(P[k - 1], conv::P_MIN)) - log(fmax(P[k], conv::P_MIN))) / conv::G;
+                const double dz = conv::RD * 0.5 * (T[k - 1] + T[k]) * (LP[k - 1] - LP[k]) / conv::G;
                 if (k >= i_lcl) cape += conv::G * fmax(buoy, 0.0) * dz;
             }
             i_lnb = n - 1;
@@ -212,19 +251,26 @@ __global__ void column_build_kernel(const ConvDev d) {
         cum[idx] = E[r] * D[c] / mb;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0) {  // the subdiagonal is a running sum: one thread, in level order
         double ce = 0.0, cd = 0.0;
         for (int k = 0; k < n - 1; ++k) {
             ce += E[k];
             cd += D[k];
             cum[(k + 1) * n + k] += fmax(ce - cd, 0.0);
         }
-        double mx = -1.0;  // CFL cap (emanuel.py:497-504)
-        for (int r = 0; r < n; ++r) {
-            double rs = 0.0;
-            for (int c = 0; c < n; ++c) rs += cum[r * n + c];
-            mx = fmax(mx, rs / fmax(M[r], 1e-12));
-        }
+    }
+    __syncthreads();
+    // CFL cap (emanuel.py:497-504): each row's outflow over its mass, one thread per row
+    // (the row summed in column order), then the largest of them
+    for (int r = tid; r < n; r += blockDim.x) {
+        double rs = 0.0;
+        for (int c = 0; c < n; ++c) rs += cum[r * n + c];
+        TVP[r] = rs / fmax(M[r], 1e-12);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double mx = -1.0;
+        for (int r = 0; r < n; ++r) mx = fmax(mx, TVP[r]);
         s_scale = (mx > conv::CFL) ? conv::CFL / mx : 1.0;
     }
     __syncthreads();
@@ -234,21 +280,18 @@ __global__ void column_build_kernel(const ConvDev d) {
     for (int k = tid; k < n; k += blockDim.x) {
         double rs = 0.0;
         for (int c = 0; c < n; ++c) rs += cum[k * n + c];
-        E[k] = fmax(fmax(M[k], 1e-6) - rs, 0.0);  // stay mass (diagonal)
+        cum[k * n + k] += fmax(fmax(M[k], 1e-6) - rs, 0.0);  // stay mass (diagonal); row k is this thread's
     }
     __syncthreads();
-    if (tid == 0) {
-        for (int k = 0; k < n; ++k) cum[k * n + k] += E[k];
-    }
-    __syncthreads();
-    // backward transition: row i = column i of fmassfrac / m_i (emanuel.py:757-759)
-    if (tid == 0) {
-        for (int r = 0; r < n; ++r)
-            for (int c = r + 1; c < n; ++c) {
-                const double a = cum[r * n + c];
-                cum[r * n + c] = cum[c * n + r];
-                cum[c * n + r] = a;
-            }
+    // backward transition: row i = column i of fmassfrac / m_i (emanuel.py:757-759); each
+    // off-diagonal pair swapped by the thread that owns its upper element
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int r = idx / n, c = idx - r * n;
+        if (c > r) {
+            const double a = cum[r * n + c];
+            cum[r * n + c] = cum[c * n + r];
+            cum[c * n + r] = a;
+        }
     }
     __syncthreads();
     for (int r = tid; r < n; r += blockDim.x) {
@@ -265,6 +308,10 @@ __global__ void column_build_kernel(const ConvDev d) {
             run += cum[r * n + c] / tot;
             cum[r * n + c] = run;
         }
+    }
+    if (matrix_in_smem) {
+        __syncthreads();
+        for (int idx = tid; idx < n * n; idx += blockDim.x) cum_out[idx] = cum[idx];
     }
 }
 
@@ -336,9 +383,7 @@ extern "C" glide_status glide_convect(const glide_convect_args* a, void* stream)
     d.n_moved = a->n_moved;
     cudaStream_t s = (cudaStream_t)stream;
     column_reduce_kernel<<<a->nz, 512, 0, s>>>(d);
-    const int threads = a->nz <= 64 ? 64 : (a->nz <= 128 ? 128 : (a->nz <= 256 ? 256 : 512));
-    const size_t smem = sizeof(double) * 10 * (size_t)a->nz;
-    column_build_kernel<<<1, threads, smem, s>>>(d);
+    column_build_kernel<<<1, kBuildThreads, column_build_smem(a->nz), s>>>(d, column_matrix_in_smem(a->nz) ? 1 : 0);
     if (a->n > 0) redistribute_kernel<<<(unsigned)((a->n + 255) / 256), 256, 0, s>>>(d);
     return check_launch("glide_convect");
 }
@@ -461,8 +506,7 @@ extern "C" glide_status glide_convect_noalloc(const glide_convect_args* a, void*
     d.n_moved = a->n_moved;
     cudaStream_t s = (cudaStream_t)stream;
     column_reduce_kernel<<<a->nz, 512, 0, s>>>(d);
-    const int threads = a->nz <= 64 ? 64 : 128;
-    column_build_kernel<<<1, threads, sizeof(double) * 10 * (size_t)a->nz, s>>>(d);
+    column_build_kernel<<<1, kBuildThreads, column_build_smem(a->nz), s>>>(d, column_matrix_in_smem(a->nz) ? 1 : 0);
     if (a->n > 0) redistribute_kernel<<<(unsigned)((a->n + 255) / 256), 256, 0, s>>>(d);
     return check_launch("glide_convect_noalloc");
 }
