@@ -516,9 +516,29 @@ class BatchRun:
             ev.record(prep_stream)
         self.prepared[k] = (wf, packed, scratch, ev)
 
+    def release(self) -> None:
+        """Per-batch reclaim (the reference's end-of-batch ``del`` + ``empty_cache``,
+        main.py:1656-1673): drop this batch's device working buffers — schedule, per-step
+        counters and diagnostic sums, particle order and work keys, convection scratch,
+        the windows prepared ahead — so that a long run's device memory stays one batch's
+        worth. What ``finish()`` handed out (the particle state, the footprint) stays
+        with its holder; ``BatchRunner.release()`` also frees the runner's packed-window
+        slots and returns the cached blocks to the driver. The batch cannot step after it."""
+        self.released = True
+        self.sched_dev = self.esc = self.act = self.diag_sum = self.wind_sum = None
+        self.order = self.work_key = self.reorder_scratch = None
+        self.keys_valid = self.order_valid = False
+        self.conv_scratch = []
+        self.prepared = {}
+        self.slot_free = [None, None]
+        self.z_edges = None
+        self.footprint = self.footprint_out = None
+
     def step_window(self, stream=None) -> bool:
         """Issue the launches of the next met window; False when the batch is done.
         Each window is an NVTX range named after its hour (for NVIDIA's profilers)."""
+        if getattr(self, "released", False):
+            raise RuntimeError("this batch was released")
         if self.done:
             return False
         torch.cuda.nvtx.range_push(f"glide window {self.steps[self.windows[self.next_window][0]].hour:%Y-%m-%dT%H}")
@@ -840,6 +860,16 @@ class BatchRunner:
             lo, hi = torch.cuda.Stream.priority_range()
             self._step_stream = torch.cuda.Stream(device=self.device, priority=hi)
         return self._step_stream
+
+    def release(self, return_to_driver: bool = True) -> None:
+        """Free the runner's packed-window slots (they are rebuilt on the next window
+        packed) and, with ``return_to_driver``, hand the blocks the caching allocator
+        keeps back to the driver (``torch.cuda.empty_cache``) — the runner-level half of
+        the per-batch reclaim, for a process that runs other work between jobs."""
+        self._slots = [None, None]
+        if return_to_driver:
+            torch.cuda.synchronize(self.device)
+            torch.cuda.empty_cache()
 
     def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:
         """The packed bricks of ``wf`` (packed into brick slot ``slot`` unless a

@@ -111,3 +111,33 @@ def test_empty_batch(cuda_device):
     assert out.status == 0
     assert out.footprint.abs().sum().item() == 0.0
     assert int(out.active_per_step.sum()) == 0
+
+
+def test_release_returns_the_batch_memory(cuda_device):
+    """Per-batch reclaim: ``BatchRun.release()`` and ``BatchRunner.release()`` free the
+    batch's working buffers, so that batch after batch on one runner the device memory
+    in use returns to the same level (no growth over a long run), and a released batch
+    refuses to step."""
+    run = load_run("run_small")
+    z = run.z
+    r = runner_for(run, cuda_device, injected=False)
+    kw = dict(batch_start=run.dt_("batch_start"), cursor_start=run.dt_("cursor_start"),
+              cursor_terminus=run.dt_("cursor_terminus"), sim_length_s=float(z["sim_length_s"]),
+              dt_seconds=float(z["dt_s"]))
+    levels, during = [], []
+    for _ in range(3):
+        st = state_from(z["particles0"], z["rel_off"], z["win_end_off"], z["release_idx"], cuda_device)
+        br = r.start(st, **kw)
+        out = br.run()
+        assert out.status == 0
+        torch.cuda.synchronize(cuda_device)
+        during.append(torch.cuda.memory_allocated(cuda_device))
+        br.release()
+        r.release()
+        with pytest.raises(RuntimeError, match="released"):
+            br.step_window()
+        del out, st, br
+        torch.cuda.synchronize(cuda_device)
+        levels.append(torch.cuda.memory_allocated(cuda_device))
+    assert levels[1] == levels[2], levels  # the same level after every batch
+    assert all(d > lv for d, lv in zip(during, levels)), (during, levels)  # the working buffers were freed
