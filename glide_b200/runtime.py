@@ -523,7 +523,8 @@ class BatchRun:
         the windows prepared ahead — so that a long run's device memory stays one batch's
         worth. What ``finish()`` handed out (the particle state, the footprint) stays
         with its holder; ``BatchRunner.release()`` also frees the runner's packed-window
-        slots and returns the cached blocks to the driver. The batch cannot step after it."""
+        slots and returns the cached blocks to the driver. The batch can neither step nor
+        finish after it."""
         self.released = True
         self.sched_dev = self.esc = self.act = self.diag_sum = self.wind_sum = None
         self.order = self.work_key = self.reorder_scratch = None
@@ -703,6 +704,8 @@ class BatchRun:
         return self.finish()
 
     def finish(self) -> BatchOutput:
+        if getattr(self, "released", False):
+            raise RuntimeError("this batch was released: finish() before release()")
         n = len(self.steps)
         status = int(self.status.item())
         fp = self.footprint if self.r.footprint.ring == 0 else self.footprint_out

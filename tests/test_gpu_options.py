@@ -136,6 +136,8 @@ def test_release_returns_the_batch_memory(cuda_device):
         r.release()
         with pytest.raises(RuntimeError, match="released"):
             br.step_window()
+        with pytest.raises(RuntimeError, match="released"):
+            br.finish()
         del out, st, br
         torch.cuda.synchronize(cuda_device)
         levels.append(torch.cuda.memory_allocated(cuda_device))
