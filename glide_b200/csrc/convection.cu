@@ -99,7 +99,9 @@ __global__ void column_reduce_kernel(const ConvDev d) {
 // Dynamic shared memory of the column build: ten per-level arrays, and the nz x nz
 // matrix too when the whole fits the default 48 KB (nz <= 73); a larger matrix is
 // built in the scratch buffer itself.
-__host__ inline bool column_matrix_in_smem(int nz) { return sizeof(double) * (10 * (size_t)nz + (size_t)nz * nz) <= 48 * 1024; }
+__host__ inline bool column_matrix_in_smem(int nz) {
+    return sizeof(double) * (10 * (size_t)nz + (size_t)nz * nz) <= 48 * 1024;
+}
 __host__ inline size_t column_build_smem(int nz) {
     return sizeof(double) * (10 * (size_t)nz + (column_matrix_in_smem(nz) ? (size_t)nz * nz : 0));
 }
