@@ -98,6 +98,29 @@ class StepPlan:
     alpha: float = 0.0
 
 
+# The step kernel's launch shape when the runner sets none: one 768-thread block per SM
+# once a batch gives every SM such a block, 128-thread blocks (six per SM) below that,
+# where the smaller blocks spread a small batch over more SMs. Measured on one B200
+# against 128 x 6: 7 % faster on the 200,000-particle single-site window, 7 % on the
+# 720-release periodic job, 6 % on the 2,688-release multisite job.
+_WIDE_SHAPE = (768, 1)
+_NARROW_SHAPE = (128, 6)
+
+
+def default_launch_variant(n_particles: int, device) -> int:
+    """Launch variant of the default shape for a batch of ``n_particles`` on ``device``."""
+    shapes = {}
+    nv = C.c_int32()
+    _abi.check(_abi.lib.glide_step_launch_variants(C.byref(nv)), "glide_step_launch_variants")
+    for v in range(nv.value - 1):  # the last variant is the general kernel at shape 0
+        t, b = C.c_int32(), C.c_int32()
+        _abi.check(_abi.lib.glide_step_launch_variant_info(v, C.byref(t), C.byref(b)), "glide_step_launch_variant_info")
+        shapes.setdefault((t.value, b.value), v)
+    sms = torch.cuda.get_device_properties(torch.device(device)).multi_processor_count
+    wide = n_particles >= sms * _WIDE_SHAPE[0] * _WIDE_SHAPE[1]
+    return shapes.get(_WIDE_SHAPE if wide else _NARROW_SHAPE, 0)
+
+
 def hour_floor(t: datetime) -> datetime:
     """main.py:380-381"""
     return t.astimezone(UTC).replace(minute=0, second=0, microsecond=0)
@@ -257,6 +280,7 @@ class BatchRun:
         self.steps = steps
         self.sim_length_s = float(sim_length_s)
         dev = runner.device
+        self._default_variant: int | None = None
         self.sched_dev = _upload(torch.from_numpy(schedule_array(steps).view(np.uint8).copy()), dev)
         self.esc = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
         self.act = torch.zeros(max(1, len(steps)), dtype=torch.int32, device=dev)
@@ -371,7 +395,12 @@ class BatchRun:
         a.active_per_step = self.act.data_ptr() + 4 * j0
         a.status = self.status.data_ptr()
         a.diag_pos_fixed = None if self.diag_sum is None else self.diag_sum.data_ptr() + 24 * j0
-        a.launch_variant = r.launch_variant
+        if r.launch_variant is not None:
+            a.launch_variant = r.launch_variant
+        else:
+            if self._default_variant is None:
+                self._default_variant = default_launch_variant(self.state.n, r.device)
+            a.launch_variant = self._default_variant
         if self.work_key is not None:
             a.order = self.order.data_ptr() if self.order_valid else None
             a.work_key = self.work_key.data_ptr()
@@ -844,7 +873,9 @@ class BatchRunner:
         # packed_provider(hour) -> PackedWindow: windows packed elsewhere and shared (read-only)
         self.packed_provider = packed_provider
         self.pipeline = bool(pipeline)
-        self.launch_variant = 0  # step-kernel launch shape (glide_b200.autotune.tune picks one)
+        # step-kernel launch shape: None = default_launch_variant(batch size);
+        # glide_b200.autotune.tune picks one for a workload
+        self.launch_variant: int | None = None
         self.reorder = True  # group particles by work class each window (results do not depend on it)
         self.steps_per_launch: int | None = None  # split each window into launches of this many steps
         self.fuse_convection = True  # convection inside the step kernel (else its own kernel between two steps)

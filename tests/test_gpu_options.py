@@ -143,3 +143,16 @@ def test_release_returns_the_batch_memory(cuda_device):
         levels.append(torch.cuda.memory_allocated(cuda_device))
     assert levels[1] == levels[2], levels  # the same level after every batch
     assert all(d > lv for d, lv in zip(during, levels)), (during, levels)  # the working buffers were freed
+
+
+def test_default_launch_shape_by_batch_size(cuda_device):
+    """Without a tuned shape the runner launches one 768-thread block per SM once the
+    batch fills every SM with such a block, and 128-thread blocks below that."""
+    from glide_b200.autotune import launch_variants
+    from glide_b200.runtime import default_launch_variant
+
+    shapes = {v: (t, b) for v, t, b in launch_variants()}
+    sms = torch.cuda.get_device_properties(cuda_device).multi_processor_count
+    assert shapes[default_launch_variant(1000, cuda_device)] == (128, 6)
+    assert shapes[default_launch_variant(sms * 768 - 1, cuda_device)] == (128, 6)
+    assert shapes[default_launch_variant(sms * 768, cuda_device)] == (768, 1)
