@@ -1,5 +1,6 @@
-"""The run configuration module: importable without the CUDA library, and the
-footprint value type checked and mapped to torch dtypes."""
+"""Host-side configuration: the run configuration module importable without the CUDA
+library, the footprint value type checked and mapped to torch dtypes, and the runtime's
+default launch shape chosen from the SM count."""
 
 from __future__ import annotations
 
@@ -33,3 +34,21 @@ def test_runtime_reexports_the_config_types():
     from glide_b200 import config, runtime
 
     assert runtime.FootprintSpec is config.FootprintSpec and runtime.HannaConfig is config.HannaConfig
+
+
+def test_default_launch_shape_follows_the_sm_count(monkeypatch):
+    """The runtime's default step-kernel shape (host logic over the library's shape
+    table, no kernel launched): one 768-thread block per SM from a batch of
+    SMs x 768 particles up, 128-thread blocks below, for any SM count."""
+    from types import SimpleNamespace
+
+    from glide_b200 import runtime
+    from glide_b200.autotune import launch_variants
+
+    shapes = {v: (t, b) for v, t, b in launch_variants()}
+    for sms in (148, 132, 20):
+        monkeypatch.setattr(torch.cuda, "get_device_properties",
+                            lambda dev, sms=sms: SimpleNamespace(multi_processor_count=sms))
+        assert shapes[runtime.default_launch_variant(sms * 768, "cuda:0")] == (768, 1)
+        assert shapes[runtime.default_launch_variant(sms * 768 - 1, "cuda:0")] == (128, 6)
+        assert shapes[runtime.default_launch_variant(0, "cuda:0")] == (128, 6)
