@@ -445,7 +445,8 @@ class BatchRun:
         with its convection fused in, from prebuilt met (``packed_provider``) and cached
         columns; nothing is launched but a missing column build. Returns the launch's
         arguments and the objects they point into (keep them until the launch has run).
-        The particle order is not used (identity)."""
+        With the runner's particle order on, the batch's particles are regrouped by the
+        work classes of its previous window (on ``stream``, before the launch)."""
         r = self.r
         if self.done:
             raise RuntimeError("the batch has no window left")
@@ -459,8 +460,10 @@ class BatchRun:
         self._record_wind_sum(k, packed, stream)
         noise = self._noise(j0, j1)
         keep = [packed, noise]
-        a = self._step_args(packed, j0, j1 - j0, 0, 0, noise)
-        a.order, a.work_key = None, None
+        if self.work_key is not None:
+            self._reorder(stream_handle(stream))
+        a = self._step_args(packed, j0, j1 - j0, 0, 0, noise)  # with the order and work keys, if any
+        self.keys_valid = self.work_key is not None  # once the caller's launch has run
         if r.emanuel is not None:
             col = self._column_for(j0, stream)
             with torch.cuda.stream(stream):

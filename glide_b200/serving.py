@@ -119,15 +119,18 @@ class FootprintServer:
     windows between ``horizon_start`` and ``horizon_end`` are packed at start-up.
     ``hbm_budget_bytes`` bounds the particle state + footprints of admitted requests,
     ``max_active`` the number of requests in flight (one CUDA stream each, from a
-    pool of ``n_streams``).
+    pool of ``n_streams``). With ``order_particles`` each request's particles are
+    regrouped by work class before every window, as the batch runtime does (results
+    do not depend on it).
     """
 
     def __init__(self, *, grid: GridInfo, met_provider, horizon_start: datetime, horizon_end: datetime,
                  hanna: HannaConfig, emanuel: EmanuelConfig | None, footprint: FootprintSpec, domain: DomainSpec,
                  hbm_budget_bytes: float = 60e9, max_active: int = 64, n_streams: int = 16, met_dtype: str = "bf16",
                  dt_seconds: float = 30.0, device="cuda", keep_footprints: bool = False,
-                 grouped: bool = True) -> None:
+                 grouped: bool = True, order_particles: bool = True) -> None:
         self.device = torch.device(device)
+        self.order_particles = bool(order_particles)
         self.grid = grid if grid.level_sorted_dev is not None else grid.to_device(self.device)
         self.hanna, self.emanuel, self.domain = hanna, emanuel, domain
         self.fp_template = footprint
@@ -175,7 +178,7 @@ class FootprintServer:
                         domain=self.domain, emanuel=self.emanuel, met_dtype=self.met_dtype, device=self.device,
                         seed=req.seed, packed_provider=lambda hour: res[hour][1])
         r.column_cache = self.column_cache
-        r.reorder = False  # small batches: the identity order
+        r.reorder = self.order_particles  # each request's particles regrouped by work class per window
         return r
 
     def _admit(self, req: FootprintRequest, now_s: float) -> None:

@@ -92,6 +92,23 @@ def test_grouped_and_per_stream_servers_agree(met):
         assert np.abs(a - b).sum() <= 1e-6 * max(np.abs(a).sum(), 1e-30)
 
 
+def test_particle_order_does_not_change_results(met):
+    """Each request's particles regrouped by work class before every window (the
+    default) or stepped in index order: the same results, grouped and per stream."""
+    syn, grid = met
+    reqs = _requests(syn)
+    for grouped in (True, False):
+        o = {r.request_id: r for r in _server(syn, grid, max_active=16, grouped=grouped).serve(reqs, realtime=False)}
+        i = {r.request_id: r for r in _server(syn, grid, max_active=16, grouped=grouped,
+                                              order_particles=False).serve(reqs, realtime=False)}
+        assert set(o) == set(i) == {r.request_id for r in reqs}
+        for k in o:
+            assert o[k].escaped == i[k].escaped and o[k].active_particle_steps == i[k].active_particle_steps
+            a, b = o[k].footprint.numpy(), i[k].footprint.numpy()
+            assert a.sum() > 0
+            assert np.abs(a - b).sum() <= 1e-6 * np.abs(a).sum()
+
+
 
 def test_budget_overfilled_with_more_than_a_grouped_launch(met, monkeypatch):
     """60 requests against a budget that holds about 40 of them: admission stops at the
