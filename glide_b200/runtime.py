@@ -556,7 +556,9 @@ class BatchRun:
         worth. What ``finish()`` handed out (the particle state, the footprint) stays
         with its holder; ``BatchRunner.release()`` also frees the runner's packed-window
         slots and returns the cached blocks to the driver. The batch can neither step nor
-        finish after it."""
+        finish after it. The device is synchronised first: a window prepared ahead on the
+        side stream, or a launch still queued, may be using the buffers."""
+        torch.cuda.synchronize(self.r.device)
         self.released = True
         self.sched_dev = self.esc = self.act = self.diag_sum = self.wind_sum = None
         self.order = self.work_key = self.reorder_scratch = None
@@ -902,10 +904,11 @@ class BatchRunner:
         """Free the runner's packed-window slots (they are rebuilt on the next window
         packed) and, with ``return_to_driver``, hand the blocks the caching allocator
         keeps back to the driver (``torch.cuda.empty_cache``) — the runner-level half of
-        the per-batch reclaim, for a process that runs other work between jobs."""
+        the per-batch reclaim, for a process that runs other work between jobs. The
+        device is synchronised first (a batch may still be packing into a slot)."""
+        torch.cuda.synchronize(self.device)
         self._slots = [None, None]
         if return_to_driver:
-            torch.cuda.synchronize(self.device)
             torch.cuda.empty_cache()
 
     def packed_for(self, wf: WindowFields, stream=None, slot: int = 0) -> PackedWindow:
